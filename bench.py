@@ -1,0 +1,355 @@
+"""Benchmark: Wilson-clover CG to a true residual |r|/|b| < 1e-10 on B200.
+
+Workload (one step = one complete solve): lattice 16^3x32, kappa = 0.1375,
+c_sw = 1.0, seeded SU(3) links exp(0.4 i H), seeded Gaussian source,
+antiperiodic in time; even-odd preconditioned CG with 16-bit inner storage,
+FP32 arithmetic and FP64 reliable updates, stopping on the FP64 true residual
+of the full system. Gauge field and source are resident in HBM when a step
+starts (`value`); `e2e` repeats the solve through the public C API with the
+source and solution in pinned HOST memory, so each step includes the
+host->device copy of b and the device->host copy of x.
+
+Printed JSON line (rank 0): metric/value (whole-job solves/s), the FP64
+solver on the same system, the roofline of the dominant kernel (the fused
+16-bit stencil, timed alone on the 32^3x64 lattice of the Dslash metric, whose
+fields exceed L2), the CPU baseline (the oracle's FP64 Schur CG on the host
+cores, a bounded sample extrapolated to a full solve), clocks sampled during
+the timed region, and the number of kernels launched.
+
+`--impl reference` times the reference path on the host cores instead (the
+reference library is GPU-only; its host-side restatement is the oracle's FP64
+CG, run with every host thread) and adds the reference library's own Dslash
+entry points timed on the GPU.
+
+Multi-GPU: the solve does not shard in this build (one lattice per GPU), so
+N ranks run N independent replicas; value = total solves / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LATTICE = (16, 16, 16, 32)
+KAPPA, CSW, EPS, BC_T, TOL = 0.1375, 1.0, 0.4, -1.0, 1e-10
+GAUGE_SEED, SOURCE_SEED = 20241, 7
+ROOF_LATTICE = (32, 32, 32, 64)
+METRIC = "CG time to |r|/|b|<1e-10, mixed vs FP64 (16^3x32 Wilson-clover, kappa 0.1375, c_sw 1)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        try:
+            for line in open(self.path):
+                f = [v.strip() for v in line.split(",")]
+                if len(f) < 7:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    mx.append(float(f[1]))
+                except ValueError:
+                    continue
+                for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = os.environ.get("QCU_BENCH_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        if device is not None and dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+def cpu_oracle_sample(U, b, L, iters_full, threads=None, s1=3, s2=9):
+    """Times the oracle's FP64 Schur CG on the host: two bounded runs (s1 and
+    s2 iterations) give the setup time and the time per iteration, which are
+    extrapolated to the iteration count of a full FP64 solve."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    t0 = time.perf_counter()
+    O.solve_schur(b, U, L, KAPPA, CSW, BC_T, TOL, s1)
+    t1 = time.perf_counter()
+    O.solve_schur(b, U, L, KAPPA, CSW, BC_T, TOL, s2)
+    t2 = time.perf_counter()
+    per_iter = max(((t2 - t1) - (t1 - t0)) / (s2 - s1), 1e-9)
+    setup = max((t1 - t0) - s1 * per_iter, 0.0)
+    full = setup + per_iter * iters_full
+    return {"solve_s": full, "per_iter_s": per_iter, "setup_s": setup, "cores": O.num_threads(),
+            "sample": f"{s1}+{s2} FP64 CG iterations of the same 16^3x32 Schur system, extrapolated to "
+                      f"{iters_full} iterations (the FP64 solve's count)"}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import qcu_cg_inverter_b200 as q
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = q.Context(LATTICE, local)
+    ctx.generate_gauge(GAUGE_SEED, EPS)
+    V = ctx.volume
+    b = torch.empty(V * 12, dtype=torch.complex128, device=device)
+    ctx.generate_spinor(b, 1, SOURCE_SEED + rank)
+    x = torch.zeros_like(b)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    kw = dict(kappa=KAPPA, csw=CSW, bc_t=BC_T, tol=TOL)
+
+    def solve(xx, bb, prec):
+        rep = ctx.invert(xx, bb, precision=prec, **kw)[0]
+        assert rep["converged"], rep
+        return rep
+
+    def timed(fn, steps):
+        """steps x fn() with an L2 flush before each, CUDA events on the library stream."""
+        total = 0.0
+        rep = None
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rep = fn()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1) / 1e3
+        return total, rep
+
+    # warm-up (also builds the clover fields and captures the CUDA graphs)
+    for _ in range(args.warmup):
+        solve(x, b, args.precision)
+    barrier(world, device)
+    torch.cuda.synchronize(device)
+    n0 = ctx.launches
+    with ClockSampler(local) as clk:
+        t_mixed, rep = timed(lambda: solve(x, b, args.precision), args.steps)
+    launches = (ctx.launches - n0) // max(args.steps, 1)
+    t_mixed = max_over_ranks(t_mixed, world, device)
+    barrier(world, device)
+    # e2e through the public C API with host buffers
+    bh = b.cpu().pin_memory()
+    xh = torch.zeros_like(bh).pin_memory()
+    solve(xh, bh, args.precision)
+    t_e2e, _ = timed(lambda: solve(xh, bh, args.precision), args.steps)
+    t_e2e = max_over_ranks(t_e2e, world, device)
+    # FP64 solver on the same system
+    solve(x, b, "double")
+    fsteps = max(1, min(args.steps, 3))
+    t_fp64, rep64 = timed(lambda: solve(x, b, "double"), fsteps)
+    t_fp64 = max_over_ranks(t_fp64, world, device)
+    # solution error of the mixed solve against the FP64 one
+    x64 = x.clone()
+    solve(x, b, args.precision)
+    err_vs_fp64 = float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64))
+
+    out = None
+    if rank == 0:
+        # dominant kernel: the fused 16-bit stencil (hop + A^-1 + xpay + second output + norm)
+        hbm, src = peaks()
+        roof = q.Context(ROOF_LATTICE, local)
+        roof.generate_gauge(GAUGE_SEED, 0.5)
+        ms, nbytes = roof.bench_stencil("half", 2, 1, 50)
+        ms_hop64, bytes_hop64 = roof.bench_stencil("double", 0, 1, 20)
+        ms_hop16, bytes_hop16 = roof.bench_stencil("half", 0, 1, 50)
+        roof.close()
+        achieved = nbytes / (ms / 1e3) / 1e9
+        # in-solve kernel at the headline size (fields L2-resident)
+        ms_small, nbytes_small = ctx.bench_stencil("half", 2, 1, 50)
+        steps = args.steps
+        per = t_mixed / steps
+        out = {
+            "metric": METRIC, "value": world * steps / t_mixed, "unit": "solves/s", "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 arithmetic, 16-bit storage, f64 reliable updates",
+            "data": "synthetic (seeded SU(3) links exp(0.4iH), seeded Gaussian source)",
+            "config": {"workload": "16^3x32 Wilson-clover even-odd CG to true residual 1e-10", "lattice": LATTICE,
+                       "kappa": KAPPA, "csw": CSW, "bc_t": "antiperiodic", "precision": args.precision,
+                       "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas x{world}"},
+            "time_to_solution_s": per, "iterations": rep["iterations"], "reliable_updates": rep["reliable_updates"],
+            "true_residual": rep["true_residual"],
+            "fp64": {"time_to_solution_s": t_fp64 / fsteps, "iterations": rep64["iterations"],
+                     "true_residual": rep64["true_residual"]},
+            "speedup_vs_fp64": (t_fp64 / fsteps) / per,
+            "solution_rel_err_vs_fp64": err_vs_fp64,
+            "e2e": {"value": world * steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": V * 12 * 16,
+                    "d2h_bytes_per_step": V * 12 * 16},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": src, "traffic": None,
+                         "kernel": "dslash half hop+A^-1+xpay+out2+norm, 32^3x64, 1 RHS",
+                         "bytes_per_launch": nbytes, "ms_per_launch": ms},
+            "dslash": {"lattice": ROOF_LATTICE,
+                       "fp64_hop_GBps": bytes_hop64 / (ms_hop64 / 1e3) / 1e9,
+                       "half_hop_GBps": bytes_hop16 / (ms_hop16 / 1e3) / 1e9,
+                       "half_fused_GBps": achieved,
+                       "in_solve_16x32_half_fused_GBps": nbytes_small / (ms_small / 1e3) / 1e9},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            U = np.zeros((4, 2, V // 2, 3, 3), complex)
+            ctx.export_gauge(U)
+            bnp = b.cpu().numpy().reshape(2, V // 2, 4, 3)
+            cb = cpu_oracle_sample(U, bnp, LATTICE, rep64["iterations"])
+            out["cpu_baseline"] = {"value": 1.0 / cb["solve_s"], "unit": "solves/s", "cores": cb["cores"],
+                                   "kind": "port", "sample": cb["sample"], "solve_s": cb["solve_s"]}
+    ctx.close()
+    return out
+
+
+def run_reference(args, world, rank, local):
+    """The reference path on the host cores (the oracle port, all threads),
+    plus the reference library's own Dslash entry points on the GPU."""
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from oracle import oracle as O
+    L = LATTICE
+    V = L[0] * L[1] * L[2] * L[3]
+    U = O.gauge_random(L, GAUGE_SEED, EPS)
+    b = O.full_spinor_random(L, SOURCE_SEED)
+    ncores = os.cpu_count() or 1
+    O.set_threads(ncores)
+    # iterations of a full FP64 solve of this system (one converged run)
+    t0 = time.perf_counter()
+    _, iters, res = O.solve_schur(b, U, L, KAPPA, CSW, BC_T, TOL, 100000)
+    t_full = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        O.solve_schur(b, U, L, KAPPA, CSW, BC_T, TOL, 2)
+    vals = []
+    for _ in range(args.steps):
+        cb = cpu_oracle_sample(U, b, L, iters, ncores)
+        vals.append(cb["solve_s"])
+    solve_s = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": 1.0 / solve_s, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded SU(3) links exp(0.4iH), seeded Gaussian source)",
+        "config": {"workload": "16^3x32 Wilson-clover even-odd CG to true residual 1e-10", "lattice": L,
+                   "kappa": KAPPA, "csw": CSW, "bc_t": "antiperiodic", "precision": "double"},
+        "cpu_baseline": {"value": 1.0 / solve_s, "unit": "solves/s", "cores": ncores, "kind": "port",
+                         "sample": cb["sample"] + f"; one full run took {t_full:.1f} s ({iters} iterations, "
+                                                  f"true residual {res:.1e})"},
+        "e2e": {"value": 1.0 / solve_s, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_note": "the reference library is GPU-only and its cg_inverter solves a different (kappa=1, "
+                          "non-Hermitian) system; the timed reference path is the oracle's FP64 restatement",
+    }
+    if os.path.exists(O.REF_LIB_PATH) and not args.no_ref_gpu:
+        try:
+            from oracle import ref_runner
+            d, _ = ref_runner.run(L, f"random:{GAUGE_SEED}:{EPS}", ["time_dslash", "time_full"], SOURCE_SEED,
+                                  timing_reps=20, timeout=900)
+            out["reference_gpu"] = {"lattice": L, "dslashQcu_ms": float(d["dslash_api_seconds"]) * 1e3,
+                                    "fullDslashQcu_ms": float(d["full_api_seconds"]) * 1e3,
+                                    "note": "reference library built for sm_100a, API-level wall time per call"}
+        except Exception as e:  # the CPU leg stands on its own
+            out["reference_gpu"] = {"error": str(e)[-300:]}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="half", choices=["half", "single", "double"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank, local)
+    else:
+        out = run_ours(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

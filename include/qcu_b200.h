@@ -1,0 +1,157 @@
+/*
+ * qcu_b200.h - extended C interface of the B200 Wilson-clover solver.
+ *
+ * Everything here returns a status code (QCU_SUCCESS = 0) instead of exiting.
+ * Two groups of entry points:
+ *
+ *  1. The reference's operator compositions, which it declares with C++
+ *     linkage in cg_inverter/include/qcu_clover_dslash.cuh:15-25 and calls
+ *     from its CG (src/qcu_clover_dslash.cu:920-1049). They use the context
+ *     created by initGridSize() and keep the reference's argument meaning.
+ *     The library also exports them under the reference's C++ symbol names,
+ *     so a binary built against the reference resolves them too.
+ *
+ *  2. New, context-based entry points for the physical operator
+ *       M = A - kappa*D,   A = 1 + kappa*c_sw*T
+ *     (T the reference's clover term, i.e. A = 1 - (kappa c_sw/2) sigma.F),
+ *     with an antiperiodic-in-time option, the even-odd preconditioned
+ *     mixed-precision CG with reliable updates, and batched multi-RHS /
+ *     multi-kappa solves. The reference has no counterpart for these; its
+ *     CG hard-codes kappa = kappa*c_sw = 1 and periodic boundaries.
+ *
+ * Field arguments are complex-double AoS spinors in the reference layout
+ * (see qcu.h). Unless stated, pointers may be device or host memory: host
+ * data is staged through device buffers inside the call.
+ */
+#ifndef QCU_B200_H
+#define QCU_B200_H
+
+#include "qcu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  QCU_SUCCESS = 0,
+  QCU_ERR_INVALID_ARG = 1,
+  QCU_ERR_CUDA = 2,
+  QCU_ERR_NOT_CONVERGED = 3,
+  QCU_ERR_OUT_OF_MEMORY = 4,
+  QCU_ERR_TIMEOUT = 5,
+  QCU_ERR_NOT_INITIALIZED = 6,
+  QCU_ERR_UNSUPPORTED = 7,
+  QCU_ERR_BREAKDOWN = 8,
+  QCU_ERR_SINGULAR_CLOVER = 9,
+  QCU_ERR_BUSY = 10
+};
+
+enum { QCU_PREC_DOUBLE = 0, QCU_PREC_SINGLE = 1, QCU_PREC_HALF = 2 };
+
+/* ---- 1. reference compositions (context from initGridSize) ---- */
+
+/* cloverDslashOneRound (src/qcu_clover_dslash.cu:990-1009):
+ * out_p = A_p^-1 D^(dag) in_{1-p} for both parities, full spinors. */
+int qcuCloverDslashOneRound(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int invert_flag);
+/* fullCloverDslashOneRound (src/qcu_clover_dslash.cu:948-987): out = (A - D^(dag)) in. */
+int qcuFullCloverDslashOneRound(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int invert_flag);
+/* newFullCloverDslashOneRound (src/qcu_clover_dslash.cu:1013-1042): out = in - A^-1 D^(dag) in. */
+int qcuNewFullCloverDslashOneRound(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int invert_flag);
+/* MmV_one_round (src/qcu_clover_dslash.cu:1044-1049):
+ * out = (1 - A^-1 D^dag)(1 - A^-1 D) in; temp is a full-spinor work buffer. */
+int qcuMmVOneRound(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, void* temp);
+/* preCloverDslash (src/qcu_clover_dslash.cu:927-944): out <- A out in place
+ * (fermion_in unused, as in the reference). */
+int qcuPreCloverDslash(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int invert_flag);
+/* cg_inverter (src/cg_inverter.cu:260-369) with its outcome returned instead
+ * of printed: iterations done and whether |<r,r>| < 1e-23 was reached. */
+int qcuCgInverterRef(void* b_vector, void* x_vector, void* gauge, QcuParam* param, int* iterations, int* converged);
+
+/* ---- 2. context-based API ---- */
+
+typedef struct qcu_context_s* qcu_context;
+
+typedef struct {
+  double kappa;       /* hopping parameter (used when the kappas array is NULL) */
+  double csw;         /* clover coefficient c_sw; 0 = plain Wilson */
+  double bc_t;        /* +1 periodic, -1 antiperiodic in time */
+  double tol;         /* target true residual |b - M x| / |b| of the full system */
+  int maxiter;        /* cap on CG iterations per right-hand side */
+  int precision;      /* inner (sloppy) precision: QCU_PREC_DOUBLE / _SINGLE / _HALF */
+  double delta;       /* reliable-update factor: the true residual is recomputed in
+                         FP64 when the iterated one fell by this factor (0 = default) */
+  int use_graphs;     /* replay CUDA graphs of the inner iterations (1 = yes) */
+} qcu_solve_params;
+
+typedef struct {
+  int iterations;        /* CG iterations on Mhat^dag Mhat */
+  int reliable_updates;  /* FP64 true-residual recomputations */
+  int converged;         /* 1 when true_residual < tol */
+  int status;            /* QCU_SUCCESS, QCU_ERR_NOT_CONVERGED or QCU_ERR_BREAKDOWN */
+  double true_residual;  /* |b - M x|/|b| of the returned x, evaluated in FP64 */
+  double kappa;
+} qcu_solve_report;
+
+/* Fills params with the defaults: kappa 0.12, csw 0, bc_t -1, tol 1e-10,
+ * maxiter 20000, precision half, delta 0.1, use_graphs 1. */
+void qcuSolveParamsDefault(qcu_solve_params* params);
+
+int qcuContextCreate(qcu_context* ctx, const int lattice[4], int device);
+int qcuContextDestroy(qcu_context ctx);
+/* Orders the context's own stream after the caller's stream (cudaStream_t):
+ * work enqueued later by the context starts after what `stream` holds now. */
+int qcuContextSetStream(qcu_context ctx, void* stream);
+/* The context's own stream (cudaStream_t), for recording events around calls. */
+void* qcuContextGetStream(qcu_context ctx);
+/* Device bytes the context holds now. */
+long long qcuContextDeviceBytes(qcu_context ctx);
+
+/* Gauge field in the reference AoS layout (device or host). */
+int qcuLoadGauge(qcu_context ctx, const void* gauge);
+/* Seeded synthetic SU(3) field U = exp(i eps H) on the device (the same
+ * counter-based streams as the CPU oracle's generator). */
+int qcuGenerateGauge(qcu_context ctx, unsigned long long seed, double eps);
+/* Copies the resident gauge field out in the AoS layout (rows 3 rebuilt). */
+int qcuExportGauge(qcu_context ctx, void* gauge_out);
+/* nrhs seeded complex-Gaussian full spinors (AoS), RHS r seeded with seed + r. */
+int qcuGenerateSpinor(qcu_context ctx, void* out, int nrhs, unsigned long long seed);
+
+/* out (half spinor, parity) = D^(dag) in (half spinor, 1-parity), hopping
+ * term with time boundary factor bc_t. */
+int qcuDslash(qcu_context ctx, void* out, const void* in, int parity, int dagger, double bc_t);
+/* out = A in (inverse = 0) or A^-1 in (inverse = 1), full spinors, with
+ * A = 1 + csw_eff*T (csw_eff = kappa*c_sw; 1 reproduces the reference). */
+int qcuApplyClover(qcu_context ctx, void* out, const void* in, double csw_eff, int inverse);
+/* out = M in or M^dag in, M = A(kappa*csw) - kappa*D, full spinors. */
+int qcuApplyOperator(qcu_context ctx, void* out, const void* in, double kappa, double csw, double bc_t, int dagger);
+
+/* Solves M x_r = b_r for nrhs right-hand sides stored back to back (full
+ * spinors). kappas (length nrhs) may be NULL to use params->kappa for all.
+ * All RHS are iterated together: each link load serves every RHS, and each
+ * RHS keeps its own CG scalars and stops on its own. reports (length nrhs)
+ * may be NULL. Returns QCU_ERR_NOT_CONVERGED if any RHS missed tol. */
+int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, const double* kappas,
+              const qcu_solve_params* params, qcu_solve_report* reports);
+
+/* Times the fused stencil kernel on resident internal fields: `variant`
+ * 0 = hop only, 1 = hop + A^-1, 2 = hop + A^-1 + xpay; precision as above;
+ * nrhs right-hand sides. Runs `iters` launches and returns the mean device
+ * time per launch in milliseconds, measured with CUDA events on the
+ * context stream; *bytes receives the algorithmic bytes of one launch. */
+int qcuBenchStencil(qcu_context ctx, int precision, int variant, int nrhs, int iters, double* ms_per_launch,
+                    double* bytes);
+
+/* Number of kernels this library enqueued since the context was created. */
+long long qcuContextLaunchCount(qcu_context ctx);
+
+/* The context behind the reference interface (NULL before initGridSize). */
+qcu_context qcuLegacyContext(void);
+
+/* Test hook for host-side fault injection: after n more successful device
+ * allocations the next one fails as out-of-memory (n < 0 disables). */
+void qcuDebugFailAllocAfter(long long n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

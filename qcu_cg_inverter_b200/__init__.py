@@ -1,0 +1,332 @@
+"""qcu_cg_inverter_b200 - B200-native Wilson-clover Dslash, clover and CG.
+
+Python binding of ``libqcu_b200.so`` (built in-tree by ``build.py``). The C
+ABI in ``include/qcu.h`` is a drop-in for the reference's ``qcu`` entry points
+(YellowBicycleee/Qcu_Cg_Inverter, cg_inverter/include/qcu.h:1-25); this module
+mirrors it with the same function names and argument meaning, so a ctypes
+front-end written for the reference calls this library the same way. Field
+arguments are CUDA tensors (complex128, reference AoS layouts) or raw device
+pointers (int).
+
+There is no CPU fallback: importing works without a GPU, but every compute
+call goes through the CUDA library and fails loudly if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libqcu_b200.so")
+
+QCU_SUCCESS = 0
+QCU_ERR_INVALID_ARG = 1
+QCU_ERR_CUDA = 2
+QCU_ERR_NOT_CONVERGED = 3
+QCU_ERR_OUT_OF_MEMORY = 4
+QCU_ERR_TIMEOUT = 5
+QCU_ERR_NOT_INITIALIZED = 6
+QCU_ERR_UNSUPPORTED = 7
+QCU_ERR_BREAKDOWN = 8
+QCU_ERR_SINGULAR_CLOVER = 9
+QCU_ERR_BUSY = 10
+
+PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
+_PREC = {"double": 0, "single": 1, "half": 2, 0: 0, 1: 1, 2: 2}
+
+
+class QcuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"qcu error {code}: {msg}")
+        self.code = code
+
+
+class QcuParam(ctypes.Structure):
+    """reference: include/qcu.h:7-9"""
+    _fields_ = [("lattice_size", ctypes.c_int * 4)]
+
+
+class QcuGrid(ctypes.Structure):
+    """reference: include/qcu.h:11-13"""
+    _fields_ = [("grid_size", ctypes.c_int * 4)]
+
+
+class SolveParams(ctypes.Structure):
+    _fields_ = [("kappa", ctypes.c_double), ("csw", ctypes.c_double), ("bc_t", ctypes.c_double),
+                ("tol", ctypes.c_double), ("maxiter", ctypes.c_int), ("precision", ctypes.c_int),
+                ("delta", ctypes.c_double), ("use_graphs", ctypes.c_int)]
+
+
+class SolveReport(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("converged", ctypes.c_int),
+                ("status", ctypes.c_int), ("true_residual", ctypes.c_double), ("kappa", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def build_library(force: bool = False) -> str:
+    """Compiles libqcu_b200.so in-tree (see build.py)."""
+    import importlib
+    return importlib.import_module(__name__ + ".build").build(force=force)
+
+
+def lib():
+    """Loads libqcu_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m qcu_cg_inverter_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        PP = ctypes.POINTER(QcuParam)
+        ll = ctypes.c_longlong
+        sig = {
+            "initGridSize": (None, [ctypes.POINTER(QcuGrid), PP, P, P, P]),
+            "dslashQcu": (None, [P, P, P, PP, i]),
+            "fullDslashQcu": (None, [P, P, P, PP, i]),
+            "cg_inverter": (None, [P, P, P, PP]),
+            "loadQcuGauge": (None, [P, PP]),
+            "invertCloverDslash": (None, [P, P, P, PP, i]),
+            "qcu_last_error": (i, []),
+            "qcu_last_error_string": (ctypes.c_char_p, []),
+            "qcuCloverDslashOneRound": (i, [P, P, P, PP, i]),
+            "qcuFullCloverDslashOneRound": (i, [P, P, P, PP, i]),
+            "qcuNewFullCloverDslashOneRound": (i, [P, P, P, PP, i]),
+            "qcuMmVOneRound": (i, [P, P, P, PP, P]),
+            "qcuPreCloverDslash": (i, [P, P, P, PP, i]),
+            "qcuCgInverterRef": (i, [P, P, P, PP, ctypes.POINTER(i), ctypes.POINTER(i)]),
+            "qcuSolveParamsDefault": (None, [ctypes.POINTER(SolveParams)]),
+            "qcuContextCreate": (i, [ctypes.POINTER(P), ctypes.POINTER(i), i]),
+            "qcuContextDestroy": (i, [P]),
+            "qcuContextSetStream": (i, [P, P]),
+            "qcuContextGetStream": (P, [P]),
+            "qcuContextDeviceBytes": (ll, [P]),
+            "qcuContextLaunchCount": (ll, [P]),
+            "qcuLoadGauge": (i, [P, P]),
+            "qcuGenerateGauge": (i, [P, ctypes.c_ulonglong, d]),
+            "qcuExportGauge": (i, [P, P]),
+            "qcuGenerateSpinor": (i, [P, P, i, ctypes.c_ulonglong]),
+            "qcuDslash": (i, [P, P, P, i, i, d]),
+            "qcuApplyClover": (i, [P, P, P, d, i]),
+            "qcuApplyOperator": (i, [P, P, P, d, d, d, i]),
+            "qcuInvert": (i, [P, P, P, i, ctypes.POINTER(d), ctypes.POINTER(SolveParams),
+                              ctypes.POINTER(SolveReport)]),
+            "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
+            "qcuDebugFailAllocAfter": (None, [ll]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error():
+    L = lib()
+    return L.qcu_last_error(), (L.qcu_last_error_string() or b"").decode()
+
+
+def _check(code: int):
+    if code != QCU_SUCCESS:
+        c, m = last_error()
+        raise QcuError(code, m)
+
+
+def _ptr(x):
+    """Device (or host) address of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    if hasattr(x, "data_ptr"):
+        assert x.is_contiguous(), "field tensors must be contiguous"
+        return ctypes.c_void_p(x.data_ptr())
+    if hasattr(x, "ctypes"):
+        assert x.flags["C_CONTIGUOUS"]
+        return ctypes.c_void_p(x.ctypes.data)
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+def param(lattice) -> QcuParam:
+    p = QcuParam()
+    for k in range(4):
+        p.lattice_size[k] = int(lattice[k])
+    return p
+
+
+# ---------------------------------------------------------------------------
+# the reference interface (include/qcu.h), same names and argument meaning
+# ---------------------------------------------------------------------------
+def initGridSize(grid, p: QcuParam, gauge, fermion_in=None, fermion_out=None) -> None:
+    """reference: src/qcu_communicator.cu:1630. grid must be (1,1,1,1)."""
+    g = QcuGrid()
+    for k in range(4):
+        g.grid_size[k] = int(grid[k])
+    lib().initGridSize(ctypes.byref(g), ctypes.byref(p), _ptr(gauge), _ptr(fermion_in), _ptr(fermion_out))
+    _check(lib().qcu_last_error())
+
+
+def loadQcuGauge(gauge, p: QcuParam) -> None:
+    """reference: src/dslash.cu:27"""
+    lib().loadQcuGauge(_ptr(gauge), ctypes.byref(p))
+    _check(lib().qcu_last_error())
+
+
+def dslashQcu(fermion_out, fermion_in, gauge, p: QcuParam, parity: int) -> None:
+    """reference: src/dslash.cu:62 - out(parity) = D in(1-parity)"""
+    lib().dslashQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(p), int(parity))
+    _check(lib().qcu_last_error())
+
+
+def fullDslashQcu(fermion_out, fermion_in, gauge, p: QcuParam, dagger_flag: int) -> None:
+    """reference: src/dslash.cu:78 - out = (A - D^(dag)) in"""
+    lib().fullDslashQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(p), int(dagger_flag))
+    _check(lib().qcu_last_error())
+
+
+def cg_inverter(b_vector, x_vector, gauge, p: QcuParam) -> None:
+    """reference: src/cg_inverter.cu:260 (its CG flow, same stopping rule)"""
+    lib().cg_inverter(_ptr(b_vector), _ptr(x_vector), _ptr(gauge), ctypes.byref(p))
+    code = lib().qcu_last_error()
+    if code not in (QCU_SUCCESS, QCU_ERR_NOT_CONVERGED):
+        _check(code)
+
+
+def invertCloverDslash(fermion_out, fermion_in, gauge, p: QcuParam, invert_flag: int = 0) -> None:
+    """reference: src/qcu_clover_dslash.cu:902 - A^-1 applied in place to out"""
+    lib().invertCloverDslash(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(p), int(invert_flag))
+    _check(lib().qcu_last_error())
+
+
+def cloverDslashOneRound(out, inp, gauge, p, invert_flag):
+    _check(lib().qcuCloverDslashOneRound(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p), int(invert_flag)))
+
+
+def fullCloverDslashOneRound(out, inp, gauge, p, invert_flag):
+    _check(lib().qcuFullCloverDslashOneRound(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p), int(invert_flag)))
+
+
+def newFullCloverDslashOneRound(out, inp, gauge, p, invert_flag):
+    _check(lib().qcuNewFullCloverDslashOneRound(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p),
+                                                int(invert_flag)))
+
+
+def MmV_one_round(out, inp, gauge, p, temp):
+    _check(lib().qcuMmVOneRound(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p), _ptr(temp)))
+
+
+def preCloverDslash(out, inp, gauge, p, invert_flag=0):
+    _check(lib().qcuPreCloverDslash(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p), int(invert_flag)))
+
+
+def cg_inverter_ref(b_vector, x_vector, gauge, p):
+    """The reference CG flow with (iterations, converged) returned."""
+    it, conv = ctypes.c_int(0), ctypes.c_int(0)
+    code = lib().qcuCgInverterRef(_ptr(b_vector), _ptr(x_vector), _ptr(gauge), ctypes.byref(p), ctypes.byref(it),
+                                  ctypes.byref(conv))
+    if code not in (QCU_SUCCESS, QCU_ERR_NOT_CONVERGED):
+        _check(code)
+    return it.value, bool(conv.value)
+
+
+# ---------------------------------------------------------------------------
+# context-based API
+# ---------------------------------------------------------------------------
+def solve_params(**kw) -> SolveParams:
+    sp = SolveParams()
+    lib().qcuSolveParamsDefault(ctypes.byref(sp))
+    for k, v in kw.items():
+        if k == "precision":
+            v = _PREC[v]
+        setattr(sp, k, v)
+    return sp
+
+
+class Context:
+    """One lattice on one GPU: resident gauge field, clover bank, solver."""
+
+    def __init__(self, lattice, device: int = 0):
+        self.lattice = tuple(int(v) for v in lattice)
+        self._h = ctypes.c_void_p()
+        L4 = (ctypes.c_int * 4)(*self.lattice)
+        _check(lib().qcuContextCreate(ctypes.byref(self._h), L4, int(device)))
+
+    def close(self):
+        if self._h:
+            lib().qcuContextDestroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def volume(self) -> int:
+        L = self.lattice
+        return L[0] * L[1] * L[2] * L[3]
+
+    def load_gauge(self, gauge):
+        _check(lib().qcuLoadGauge(self._h, _ptr(gauge)))
+
+    def generate_gauge(self, seed: int, eps: float):
+        _check(lib().qcuGenerateGauge(self._h, int(seed), float(eps)))
+
+    def export_gauge(self, out):
+        _check(lib().qcuExportGauge(self._h, _ptr(out)))
+
+    def generate_spinor(self, out, nrhs: int, seed: int):
+        _check(lib().qcuGenerateSpinor(self._h, _ptr(out), int(nrhs), int(seed)))
+
+    def dslash(self, out, inp, parity: int, dagger: int = 0, bc_t: float = 1.0):
+        _check(lib().qcuDslash(self._h, _ptr(out), _ptr(inp), int(parity), int(dagger), float(bc_t)))
+
+    def apply_clover(self, out, inp, csw_eff: float, inverse: bool):
+        _check(lib().qcuApplyClover(self._h, _ptr(out), _ptr(inp), float(csw_eff), int(bool(inverse))))
+
+    def apply_operator(self, out, inp, kappa: float, csw: float, bc_t: float = -1.0, dagger: int = 0):
+        _check(lib().qcuApplyOperator(self._h, _ptr(out), _ptr(inp), float(kappa), float(csw), float(bc_t),
+                                      int(dagger)))
+
+    def invert(self, x, b, nrhs: int = 1, kappas=None, raise_on_fail: bool = True, **kw):
+        sp = solve_params(**kw)
+        reps = (SolveReport * nrhs)()
+        karr = None
+        if kappas is not None:
+            karr = (ctypes.c_double * nrhs)(*[float(k) for k in kappas])
+        code = lib().qcuInvert(self._h, _ptr(x), _ptr(b), int(nrhs), karr, ctypes.byref(sp), reps)
+        if code != QCU_SUCCESS and (raise_on_fail or code not in (QCU_ERR_NOT_CONVERGED, QCU_ERR_BREAKDOWN)):
+            _check(code)
+        return [r.as_dict() for r in reps]
+
+    def bench_stencil(self, precision, variant: int, nrhs: int = 1, iters: int = 20):
+        ms, nbytes = ctypes.c_double(0), ctypes.c_double(0)
+        _check(lib().qcuBenchStencil(self._h, _PREC[precision], int(variant), int(nrhs), int(iters),
+                                     ctypes.byref(ms), ctypes.byref(nbytes)))
+        return ms.value, nbytes.value
+
+    @property
+    def stream(self) -> int:
+        """Address of the context's cudaStream_t (wrap with torch.cuda.ExternalStream)."""
+        return int(lib().qcuContextGetStream(self._h) or 0)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().qcuContextLaunchCount(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().qcuContextDeviceBytes(self._h))

@@ -1,0 +1,75 @@
+// Device-resident CG scalars, one entry per right-hand side, and the finishing
+// functors that update them at the end of a fused reduction (executed by one
+// thread of the last block, so no host round trip is needed per iteration).
+//
+// Iteration of the sloppy CG on N = Mhat^dag Mhat (per RHS r):
+//   y = Mhat p, pAp = |y|^2           -> FinCgAlpha: alpha = rr / pAp
+//   z = Mhat^dag y
+//   x += alpha p, r -= alpha z, rr' = |r|^2
+//                                     -> FinCgBeta:  beta = rr'/rr, rr = rr';
+//                                        pauses the RHS (active = 0, event = 1)
+//                                        when rr' < trigger (reliable update or
+//                                        convergence check due)
+//   p = r + beta p
+// The reference computes alpha and beta on the host after two blocking copies
+// per dot product (src/cg_inverter.cu:204-235); here they never leave the GPU.
+#pragma once
+#include "qcu_common.cuh"
+
+namespace qcu {
+
+struct CgDevState {
+  double* rr;       // |r|^2 of the iterated residual
+  double* rr_old;   // |r|^2 before the last update (for beta after a reliable update)
+  double* pAp;
+  double* alpha;
+  double* beta;
+  double* trigger;  // pause when rr < trigger
+  int* active;      // 1 while the RHS iterates
+  int* event;       // set when the RHS paused itself
+  int* iters;
+  int* breakdown;   // set when pAp <= 0 or not finite
+};
+
+struct FinCgAlpha {
+  static QCU_D void apply(const double* res, int nrhs, int NR, void* st) {
+    CgDevState* s = static_cast<CgDevState*>(st);
+    for (int r = 0; r < nrhs; r++) {
+      if (!s->active[r]) continue;
+      double pap = res[r * NR];
+      s->pAp[r] = pap;
+      if (!(pap > 0.0) || !isfinite(pap)) {
+        s->breakdown[r] = 1;
+        s->active[r] = 0;
+        s->event[r] = 1;
+        s->alpha[r] = 0.0;
+      } else {
+        s->alpha[r] = s->rr[r] / pap;
+      }
+    }
+  }
+};
+
+struct FinCgBeta {
+  static QCU_D void apply(const double* res, int nrhs, int NR, void* st) {
+    CgDevState* s = static_cast<CgDevState*>(st);
+    for (int r = 0; r < nrhs; r++) {
+      if (!s->active[r]) continue;
+      double rn = res[r * NR];
+      s->beta[r] = rn / s->rr[r];
+      s->rr_old[r] = s->rr[r];
+      s->rr[r] = rn;
+      s->iters[r] += 1;
+      if (!isfinite(rn)) {
+        s->breakdown[r] = 1;
+        s->active[r] = 0;
+        s->event[r] = 1;
+      } else if (rn < s->trigger[r]) {
+        s->active[r] = 0;
+        s->event[r] = 1;
+      }
+    }
+  }
+};
+
+}  // namespace qcu

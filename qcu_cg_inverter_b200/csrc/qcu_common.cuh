@@ -1,0 +1,190 @@
+// Common device/host definitions for the B200 Wilson-clover solver.
+//
+// Conventions (they follow the reference library, YellowBicycleee/Qcu_Cg_Inverter,
+// paths below are inside its cg_inverter/ directory):
+//  * even-odd checkerboard: parity p holds sites with (x+y+z+t)&1 == p; the
+//    checkerboard index is s = ((t*Lz + z)*Ly + y)*(Lx/2) + x/2 and the full x
+//    coordinate is x = 2*(x/2) + ((y+z+t+p)&1) (include/qcu_point.cuh:20-72);
+//  * spinor component k = spin*3 + colour, DeGrand-Rossi gamma basis as written
+//    out in the hopping kernel (src/qcu_clover_dslash.cu:570-772);
+//  * links keep their first two rows; the third is conj(row0 x row1)
+//    (src/qcu_clover_dslash.cu:11-16);
+//  * the clover matrix of a site is two 6x6 Hermitian blocks acting on spins
+//    {0,1} and {2,3} (src/qcu_clover_dslash.cu:461-506).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <cuda_fp16.h>
+
+#define QCU_HD __host__ __device__ __forceinline__
+#define QCU_D __device__ __forceinline__
+
+namespace qcu {
+
+// ---------------------------------------------------------------------------
+// complex arithmetic
+// ---------------------------------------------------------------------------
+template <class R> struct Cplx {
+  R re, im;
+};
+template <class R> QCU_HD Cplx<R> mk(R a, R b) { return Cplx<R>{a, b}; }
+template <class R> QCU_HD Cplx<R> operator+(Cplx<R> a, Cplx<R> b) { return {a.re + b.re, a.im + b.im}; }
+template <class R> QCU_HD Cplx<R> operator-(Cplx<R> a, Cplx<R> b) { return {a.re - b.re, a.im - b.im}; }
+template <class R> QCU_HD Cplx<R> operator*(Cplx<R> a, Cplx<R> b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <class R> QCU_HD Cplx<R> operator*(R s, Cplx<R> a) { return {s * a.re, s * a.im}; }
+template <class R> QCU_HD Cplx<R> conj(Cplx<R> a) { return {a.re, -a.im}; }
+template <class R> QCU_HD Cplx<R> mul_i(Cplx<R> a) { return {-a.im, a.re}; }  // i*a
+template <class R> QCU_HD Cplx<R>& operator+=(Cplx<R>& a, Cplx<R> b) { a.re += b.re; a.im += b.im; return a; }
+template <class R> QCU_HD Cplx<R>& operator-=(Cplx<R>& a, Cplx<R> b) { a.re -= b.re; a.im -= b.im; return a; }
+// a += b*c
+template <class R> QCU_HD void cmac(Cplx<R>& a, Cplx<R> b, Cplx<R> c) {
+  a.re += b.re * c.re - b.im * c.im;
+  a.im += b.re * c.im + b.im * c.re;
+}
+// a += conj(b)*c
+template <class R> QCU_HD void cmac_conj(Cplx<R>& a, Cplx<R> b, Cplx<R> c) {
+  a.re += b.re * c.re + b.im * c.im;
+  a.im += b.re * c.im - b.im * c.re;
+}
+
+template <class R> struct Spinor {
+  Cplx<R> c[12];  // spin*3 + colour
+};
+template <class R> struct Link {
+  Cplx<R> u[9];   // row-major 3x3
+};
+
+template <class R> QCU_HD void su3_reconstruct(Link<R>& L) {
+  // row 3 = conj(row1 x row2)
+  L.u[6] = conj(L.u[1] * L.u[5] - L.u[2] * L.u[4]);
+  L.u[7] = conj(L.u[2] * L.u[3] - L.u[0] * L.u[5]);
+  L.u[8] = conj(L.u[0] * L.u[4] - L.u[1] * L.u[3]);
+}
+
+// ---------------------------------------------------------------------------
+// lattice geometry
+// ---------------------------------------------------------------------------
+struct Geom {
+  int Lx, Ly, Lz, Lt;
+  int Lxh;      // Lx/2
+  int Vh;       // sites per parity
+  int Vh_pad;   // Vh rounded up to the 32-site block
+  int sy, sz, st;  // checkerboard strides of y, z, t: Lxh, Lxh*Ly, Lxh*Ly*Lz
+};
+
+inline Geom make_geom(const int L[4]) {
+  Geom g;
+  g.Lx = L[0]; g.Ly = L[1]; g.Lz = L[2]; g.Lt = L[3];
+  g.Lxh = L[0] / 2;
+  g.Vh = g.Lxh * g.Ly * g.Lz * g.Lt;
+  g.Vh_pad = (g.Vh + 31) & ~31;
+  g.sy = g.Lxh;
+  g.sz = g.Lxh * g.Ly;
+  g.st = g.Lxh * g.Ly * g.Lz;
+  return g;
+}
+
+// Coordinates and the 8 neighbours of a checkerboard site. The x step follows
+// Point::move (include/qcu_point.cuh:26-36): with eo = (y+z+t)&1 the forward
+// x neighbour has x/2+1 when eo != parity (else the same x/2), the backward
+// one x/2-1 when eo == parity; every direction wraps periodically.
+struct Nbrs {
+  int fwd[4], bwd[4];
+  int t;   // time coordinate (for the t boundary phase)
+};
+
+QCU_HD Nbrs neighbours(const Geom& g, int s, int parity) {
+  Nbrs n;
+  int xh = s % g.Lxh;
+  int r = s / g.Lxh;
+  int y = r % g.Ly;
+  r /= g.Ly;
+  int z = r % g.Lz;
+  int t = r / g.Lz;
+  n.t = t;
+  int eo = (y + z + t) & 1;
+  int xf = (eo != parity) ? (xh + 1 == g.Lxh ? 0 : xh + 1) : xh;
+  int xb = (eo == parity) ? (xh == 0 ? g.Lxh - 1 : xh - 1) : xh;
+  n.fwd[0] = s - xh + xf;
+  n.bwd[0] = s - xh + xb;
+  n.fwd[1] = (y + 1 == g.Ly) ? s - (g.Ly - 1) * g.sy : s + g.sy;
+  n.bwd[1] = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
+  n.fwd[2] = (z + 1 == g.Lz) ? s - (g.Lz - 1) * g.sz : s + g.sz;
+  n.bwd[2] = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
+  n.fwd[3] = (t + 1 == g.Lt) ? s - (g.Lt - 1) * g.st : s + g.st;
+  n.bwd[3] = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// internal field layout: site-blocked, vectorised SoA
+// ---------------------------------------------------------------------------
+// Every field is a sequence of 16-byte chunks. Sites are grouped in blocks of
+// 32 (one warp); within a block, chunk c of all 32 sites (and, for batched
+// fields, of all nrhs right-hand sides of each site) is contiguous:
+//     chunk(c, s, r) = ((s/32 * NC + c) * 32 + s%32) * nrhs + r
+// so a warp reading chunk c of 32 consecutive sites reads 512*nrhs contiguous
+// bytes, and all chunks of a site block sit within a few KB.
+QCU_HD size_t chunk_index(int c, int s, int r, int NC, int nrhs) {
+  return ((size_t)((s >> 5) * NC + c) * 32 + (s & 31)) * (size_t)nrhs + r;
+}
+
+// ---------------------------------------------------------------------------
+// precision traits
+// ---------------------------------------------------------------------------
+enum Prec : int { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
+
+// 16-bit storage is fixed point: a real v in [-1,1] is stored as
+// round(v*32767); spinors and clover blocks carry one float norm per site so
+// that their largest component maps to 1.
+constexpr float kFix = 32767.0f;
+constexpr float kInvFix = 1.0f / 32767.0f;
+
+// spinor chunks per site: 12 complex in 16 bytes
+template <int P> struct SpinorChunks;
+template <> struct SpinorChunks<PREC_DOUBLE> { static constexpr int NC = 12; };  // double2
+template <> struct SpinorChunks<PREC_SINGLE> { static constexpr int NC = 6; };   // float4
+template <> struct SpinorChunks<PREC_HALF> { static constexpr int NC = 3; };     // 8 x int16
+// gauge: 12 reals per link
+template <int P> struct GaugeChunks;
+template <> struct GaugeChunks<PREC_DOUBLE> { static constexpr int NC = 6; };   // double2
+template <> struct GaugeChunks<PREC_SINGLE> { static constexpr int NC = 3; };   // float4
+template <> struct GaugeChunks<PREC_HALF> { static constexpr int NC = 3; };     // 4 x int16 (8 bytes)
+// packed clover: 72 reals per site (two Hermitian 6x6 blocks, 36 reals each:
+// 6 real diagonal entries, then the 15 strictly-lower entries row by row)
+template <int P> struct CloverChunks;
+template <> struct CloverChunks<PREC_DOUBLE> { static constexpr int NC = 36; };  // double2
+template <> struct CloverChunks<PREC_SINGLE> { static constexpr int NC = 18; };  // float4
+template <> struct CloverChunks<PREC_HALF> { static constexpr int NC = 9; };     // 8 x int16
+
+template <int P> struct CompReal { typedef float type; };
+template <> struct CompReal<PREC_DOUBLE> { typedef double type; };
+
+// bytes per site of each field kind
+template <int P> constexpr int spinor_bytes() { return P == PREC_DOUBLE ? 192 : (P == PREC_SINGLE ? 96 : 52); }
+template <int P> constexpr int link_bytes() { return P == PREC_DOUBLE ? 96 : (P == PREC_SINGLE ? 48 : 24); }
+template <int P> constexpr int clover_bytes() { return P == PREC_DOUBLE ? 576 : (P == PREC_SINGLE ? 288 : 148); }
+
+// off-diagonal packed index of (i,j), i > j, of a 6x6 Hermitian block
+QCU_HD int tri_index(int i, int j) { return i * (i - 1) / 2 + j; }
+
+// ---------------------------------------------------------------------------
+// counter-based random numbers (SplitMix64 streams keyed by (seed, object))
+// ---------------------------------------------------------------------------
+QCU_HD uint64_t sm64_next(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+QCU_HD uint64_t stream_init(uint64_t seed, uint64_t object) {
+  uint64_t s = seed ^ 0xD1B54A32D192ED03ull;
+  s += object * 0x632BE59BD9B4E019ull;
+  (void)sm64_next(s);
+  return s;
+}
+
+}  // namespace qcu

@@ -1,0 +1,179 @@
+// Host-side state of the library: device buffers, the resident gauge field,
+// the bank of factored clover fields, reduction scratch and the error
+// channel. Replaces the reference's process globals (static clover and
+// inverse, src/qcu_clover_dslash.cu:564-568; qcu_gauge, src/dslash.cu:26;
+// mpi_comm, src/qcu_communicator.cu:1031) by an explicit context.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/qcu_b200.h"
+#include "qcu_cg_state.cuh"
+#include "qcu_common.cuh"
+#include "qcu_fields.cuh"
+#include "qcu_kernels.cuh"
+
+namespace qcu {
+
+// ---------------- errors ----------------
+void set_error(int code, const std::string& msg);
+void clear_error();
+int last_error();
+
+// converts a CUDA error into a status (and records it)
+int cuda_status(cudaError_t e, const char* what);
+
+#define QCU_CHECK_CUDA(expr)                                       \
+  do {                                                             \
+    cudaError_t _e = (expr);                                       \
+    if (_e != cudaSuccess) return ::qcu::cuda_status(_e, #expr);   \
+  } while (0)
+#define QCU_CHECK(expr)                \
+  do {                                 \
+    int _s = (expr);                   \
+    if (_s != QCU_SUCCESS) return _s;  \
+  } while (0)
+
+// ---------------- device memory ----------------
+// Test hook: after `n` more successful allocations the next one fails
+// (negative n = never). Used by the host-side fault tests.
+void set_alloc_fail_after(long long n);
+cudaError_t dev_alloc(void** p, size_t bytes);
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  // (re)allocates to at least `n` bytes, zero-filled
+  int ensure(size_t n, cudaStream_t st);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() { release(); }
+  int ensure(size_t n);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------- spinor fields ----------------
+struct Field {
+  int prec = PREC_DOUBLE;
+  int nrhs = 0;
+  int nsites = 0;  // sites per parity block (Vh_pad)
+  int nparity = 1;
+  DevBuf data, norm;
+  int alloc(int prec_, int nsites_, int nrhs_, int nparity_, cudaStream_t st);
+  SpinorView view(int parity = 0) const;
+  CSpinorView cview(int parity = 0) const { return CSpinorView(view(parity)); }
+  size_t parity_bytes() const { return spinor_field_bytes(prec, nsites, nrhs); }
+  size_t parity_norm_bytes() const { return spinor_norm_bytes(prec, nsites, nrhs); }
+};
+
+// ---------------- clover bank ----------------
+// Factored clover fields for several values of csw_eff = kappa*c_sw, each
+// slot holding A (FP64) and A^-1 (FP64, single, 16-bit), all slots of one
+// precision in one allocation so that a kernel can address slot k as
+// base + k*stride (one right-hand side per kappa in a batch).
+struct CloverBank {
+  int capacity = 0;
+  size_t b64 = 0, b32 = 0, b16 = 0;
+  DevBuf A64, Ainv64, Ainv32, Ainv16;
+  std::vector<double> csw;       // csw_eff of each slot (NaN = free)
+  std::vector<long long> stamp;  // last use, for eviction
+  std::vector<int> pinned;       // slots used by the batch being prepared
+};
+
+struct Scratch {
+  DevBuf partial, ticket, result;
+  PinnedBuf host;
+  size_t partial_doubles = 0;
+  int ensure(const Geom& g, int nrhs, cudaStream_t st);
+  ReduceArgs args(void* state = nullptr) const {
+    return ReduceArgs{partial.as<double>(), ticket.as<unsigned>(), result.as<double>(), state};
+  }
+};
+
+struct SolverWorkspace;  // solver.cu
+
+}  // namespace qcu
+
+struct qcu_context_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int L[4] = {0, 0, 0, 0};
+  qcu::Geom g{};
+  // resident gauge field (internal layout) in three precisions
+  qcu::DevBuf gauge64, gauge32, gauge16;
+  bool gauge_loaded = false;
+  long long gauge_version = 0;
+  const void* legacy_gauge_src = nullptr;  // AoS pointer last ingested by the legacy API
+  qcu::CloverBank clover;
+  long long clock = 0;
+  qcu::Scratch red;
+  qcu::LaunchShape shape1{1, 128};  // single-RHS stencil/BLAS shape
+  // scratch fields for the legacy and operator entry points
+  qcu::Field lin, lout, ltmp, ltmp2, lx;
+  qcu::DevBuf stage_in, stage_out;  // device staging of host arguments
+  qcu::DevBuf status;               // clover build status counters
+  qcu::SolverWorkspace* solver = nullptr;  // owned; freed by qcuContextDestroy (solver.cu)
+  long long launches = 0;
+  ~qcu_context_s();
+};
+
+namespace qcu {
+
+// context helpers (api.cu)
+int ctx_check(qcu_context ctx);
+int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot);  // builds on demand
+int ctx_clover_reserve(qcu_context ctx, int nslots);
+const void* ctx_clover_ptr(qcu_context ctx, int prec, bool inverse);
+size_t ctx_clover_stride(qcu_context ctx, int prec);
+const void* ctx_gauge(qcu_context ctx, int prec);
+
+// staging of user pointers that may live on the host
+bool is_device_ptr(const void* p);
+
+// kernel launchers (defined in the .cu files)
+cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, cudaStream_t st);
+cudaError_t launch_spinor_in(int prec, const Geom& g, int nrhs, const void* aos, size_t aos_stride, SpinorView dst,
+                             cudaStream_t st);
+cudaError_t launch_spinor_out(int prec, const Geom& g, int nrhs, CSpinorView src, void* aos, size_t aos_stride,
+                              cudaStream_t st);
+cudaError_t launch_gauge_random(const Geom& g, uint64_t seed, double eps, void* aos, cudaStream_t st);
+cudaError_t launch_spinor_random(size_t nsites, uint64_t seed, void* aos, cudaStream_t st);
+cudaError_t launch_clover_build(const Geom& g, const void* gauge64, double csw_eff, void* A64, void* Ainv64,
+                                void* Ainv32, void* Ainv16, int* status, cudaStream_t stream);
+cudaError_t launch_clover_apply(int prec, const Geom& g, int parity, int nrhs, CSpinorView in, SpinorView out,
+                                const void* clov, size_t clov_stride, const int* clov_idx, const int* active,
+                                const ReduceArgs* red, LaunchShape sh, cudaStream_t stream);
+cudaError_t launch_cg_xr(int pa, int ps, int nsites, int nrhs, SpinorView x, SpinorView r, CSpinorView p, CSpinorView z,
+                         const double* alpha, const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_cg_p(int pa, int ps, int nsites, int nrhs, SpinorView p, CSpinorView r, const double* beta,
+                        const int* active, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_convert(int pd, int psrc, int nsites, int nrhs, SpinorView dst, CSpinorView src, const int* active,
+                           const ReduceArgs* red, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_accumulate(int pl, int nsites, int nrhs, SpinorView xhi, SpinorView xlo, const int* active,
+                              LaunchShape sh, cudaStream_t st);
+cudaError_t launch_residual(int nsites, int nrhs, SpinorView r, CSpinorView b, CSpinorView z, const int* active,
+                            const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_cdot(int prec, int nsites, int nrhs, CSpinorView x, CSpinorView y, const int* active,
+                        const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_ref_xr(int nsites, SpinorView x, CSpinorView p, CSpinorView r, CSpinorView ap, SpinorView r2,
+                          double2 a, const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
+cudaError_t launch_ref_p(int nsites, SpinorView p, CSpinorView r2, double2 b, LaunchShape sh, cudaStream_t st);
+
+}  // namespace qcu

@@ -1,0 +1,135 @@
+// The Wilson hopping term on one checkerboard, as a device function shared by
+// all stencil kernels.
+//
+//   out(x) = sum_mu (1 - f g_mu) U_mu(x) in(x+mu) + (1 + f g_mu) U_mu(x-mu)^dag in(x-mu)
+//
+// f = +1 (D) or -1 (D^dag, which is exactly the adjoint of D), DeGrand-Rossi
+// gamma matrices. Each direction is a two-component spin projection, two SU(3)
+// mat-vecs and the spin reconstruction, with the same projector rows as the
+// reference hopping kernel (src/qcu_clover_dslash.cu:599-768, flag = f). The
+// reference has no kappa and no overall sign; neither has this function.
+// bc_t multiplies every hop that crosses the t boundary (-1: antiperiodic).
+#pragma once
+#include "qcu_fields.cuh"
+
+namespace qcu {
+
+template <class R> struct Half2 {
+  Cplx<R> h0[3], h1[3];
+};
+
+// h = P_mu^{fwd/bwd} psi. FWD: (1 - F g_mu), BWD: (1 + F g_mu).
+template <int MU, bool FWD, int F, class R>
+QCU_D void project(Half2<R>& h, const Spinor<R>& p) {
+  // sign of the projector term: S = -F forward, +F backward
+  constexpr int S = FWD ? -F : F;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const Cplx<R> p0 = p.c[c], p1 = p.c[3 + c], p2 = p.c[6 + c], p3 = p.c[9 + c];
+    if constexpr (MU == 0) {  // h0 = p0 + S i p3, h1 = p1 + S i p2
+      h.h0[c] = S > 0 ? p0 + mul_i(p3) : p0 - mul_i(p3);
+      h.h1[c] = S > 0 ? p1 + mul_i(p2) : p1 - mul_i(p2);
+    } else if constexpr (MU == 1) {  // h0 = p0 - S p3, h1 = p1 + S p2
+      h.h0[c] = S > 0 ? p0 - p3 : p0 + p3;
+      h.h1[c] = S > 0 ? p1 + p2 : p1 - p2;
+    } else if constexpr (MU == 2) {  // h0 = p0 + S i p2, h1 = p1 - S i p3
+      h.h0[c] = S > 0 ? p0 + mul_i(p2) : p0 - mul_i(p2);
+      h.h1[c] = S > 0 ? p1 - mul_i(p3) : p1 + mul_i(p3);
+    } else {  // h0 = p0 + S p2, h1 = p1 + S p3
+      h.h0[c] = S > 0 ? p0 + p2 : p0 - p2;
+      h.h1[c] = S > 0 ? p1 + p3 : p1 - p3;
+    }
+  }
+}
+
+// out += reconstruct(a = U h0, b = U h1)
+template <int MU, bool FWD, int F, class R>
+QCU_D void reconstruct(Spinor<R>& o, const Cplx<R> a[3], const Cplx<R> b[3]) {
+  constexpr int S = FWD ? -F : F;  // same sign convention as project()
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.c[c] += a[c];
+    o.c[3 + c] += b[c];
+    if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a
+      if (S > 0) { o.c[6 + c] -= mul_i(b[c]); o.c[9 + c] -= mul_i(a[c]); }
+      else { o.c[6 + c] += mul_i(b[c]); o.c[9 + c] += mul_i(a[c]); }
+    } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a
+      if (S > 0) { o.c[6 + c] += b[c]; o.c[9 + c] -= a[c]; }
+      else { o.c[6 + c] -= b[c]; o.c[9 + c] += a[c]; }
+    } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b
+      if (S > 0) { o.c[6 + c] -= mul_i(a[c]); o.c[9 + c] += mul_i(b[c]); }
+      else { o.c[6 + c] += mul_i(a[c]); o.c[9 + c] -= mul_i(b[c]); }
+    } else {  // o2 += S a, o3 += S b
+      if (S > 0) { o.c[6 + c] += a[c]; o.c[9 + c] += b[c]; }
+      else { o.c[6 + c] -= a[c]; o.c[9 + c] -= b[c]; }
+    }
+  }
+}
+
+template <class R>
+QCU_D void su3_mul(Cplx<R> o[3], const Link<R>& U, const Cplx<R> v[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    Cplx<R> acc = U.u[i * 3] * v[0];
+    cmac(acc, U.u[i * 3 + 1], v[1]);
+    cmac(acc, U.u[i * 3 + 2], v[2]);
+    o[i] = acc;
+  }
+}
+template <class R>
+QCU_D void su3_dag_mul(Cplx<R> o[3], const Link<R>& U, const Cplx<R> v[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    Cplx<R> acc = mk(R(0), R(0));
+    cmac_conj(acc, U.u[i], v[0]);
+    cmac_conj(acc, U.u[3 + i], v[1]);
+    cmac_conj(acc, U.u[6 + i], v[2]);
+    o[i] = acc;
+  }
+}
+
+template <class R> QCU_D void scale_half(Half2<R>& h, R s) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) { h.h0[c] = s * h.h0[c]; h.h1[c] = s * h.h1[c]; }
+}
+
+// One direction (both hops) of the stencil.
+template <int P, int MU, int F, class R>
+QCU_D void hop_dir(Spinor<R>& o, const Geom& g, const Nbrs& nb, int parity, int s, int r,
+                   const CSpinorView& in, const void* gauge, R bc_t) {
+  Link<R> U;
+  Spinor<R> p;
+  Half2<R> h;
+  Cplx<R> a[3], b[3];
+  // forward: U_mu(x) in(x+mu)
+  LinkIO<P>::load(U, gauge, g.Vh_pad, MU, parity, s);
+  SpinorIO<P>::load(p, in, nb.fwd[MU], r);
+  project<MU, true, F>(h, p);
+  if (MU == 3 && nb.t == g.Lt - 1) scale_half(h, bc_t);
+  su3_mul(a, U, h.h0);
+  su3_mul(b, U, h.h1);
+  reconstruct<MU, true, F>(o, a, b);
+  // backward: U_mu(x-mu)^dag in(x-mu); the link lives on the other parity
+  LinkIO<P>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
+  SpinorIO<P>::load(p, in, nb.bwd[MU], r);
+  project<MU, false, F>(h, p);
+  if (MU == 3 && nb.t == 0) scale_half(h, bc_t);
+  su3_dag_mul(a, U, h.h0);
+  su3_dag_mul(b, U, h.h1);
+  reconstruct<MU, false, F>(o, a, b);
+}
+
+template <int P, bool DAG, class R>
+QCU_D void hop(Spinor<R>& o, const Geom& g, int parity, int s, int r, const CSpinorView& in,
+               const void* gauge, R bc_t) {
+  constexpr int F = DAG ? -1 : 1;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.c[k] = mk(R(0), R(0));
+  const Nbrs nb = neighbours(g, s, parity);
+  hop_dir<P, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<P, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<P, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<P, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+}
+
+}  // namespace qcu

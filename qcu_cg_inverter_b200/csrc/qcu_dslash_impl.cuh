@@ -1,0 +1,82 @@
+// Fused Wilson-clover stencil kernels: hop + optional clover, xpay, second
+// output and per-RHS norm reduction, for double, single and 16-bit storage.
+//
+// One thread per (site, right-hand side). Threads of a warp that share a site
+// (rhs lanes, threadIdx.x) load the same link addresses, which the memory
+// system serves once; adjacent rhs lanes read adjacent spinor chunks.
+#pragma once
+#include "qcu_cg_state.cuh"
+#include "qcu_dslash.cuh"
+#include "qcu_kernels.cuh"
+
+namespace qcu {
+
+typedef void (*DslashKernelFn)(const DslashArgs);
+
+template <int P, bool DAG, int EPI, class Fin>
+__global__ void __launch_bounds__(256) dslash_kernel(const DslashArgs a) {
+  typedef typename CompReal<P>::type R;
+  const int r = blockIdx.y * blockDim.x + threadIdx.x;
+  const int s = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool valid = (s < a.g.Vh) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
+  double nrm = 0.0;
+  if (valid) {
+    Spinor<R> o;
+    hop<P, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
+    const void* clov = a.clover;
+    if (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) {
+      if (a.clover_idx) clov = static_cast<const char*>(a.clover) + a.clover_stride * (size_t)a.clover_idx[r];
+    }
+    if (EPI & EPI_CPRE) clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
+    if (EPI & EPI_XPAY) {
+      const R c = a.coef ? (R)a.coef[r] : (R)a.coef0;
+      Spinor<R> xv;
+      SpinorIO<P>::load(xv, a.x, s, r);
+      if (EPI & EPI_CX) clover_apply_site<P>(xv, clov, a.g.Vh_pad, a.parity, s);
+#pragma unroll
+      for (int k = 0; k < 12; k++) o.c[k] = xv.c[k] + c * o.c[k];
+      if (EPI & EPI_CPOST) clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
+    }
+    SpinorIO<P>::store(a.out, s, r, o);
+    if (EPI & EPI_NORM) {
+#pragma unroll
+      for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
+    }
+    if (EPI & EPI_OUT2) {
+      clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
+      SpinorIO<P>::store(a.out2, s, r, o);
+    }
+  }
+  if (EPI & EPI_NORM) {
+    double v[1] = {nrm};
+    block_reduce_finish<1, Fin>(v, a.nrhs, a.red);
+  }
+}
+
+template <int P, bool DAG>
+static DslashKernelFn pick(int epi, int fin) {
+#define QCU_CASE(E)                                                                     \
+  case (E):                                                                             \
+    if ((E)&EPI_NORM) {                                                                 \
+      if (fin == FIN_CG_ALPHA) return dslash_kernel<P, DAG, (E), FinCgAlpha>;           \
+      return dslash_kernel<P, DAG, (E), FinNone>;                                       \
+    }                                                                                   \
+    return dslash_kernel<P, DAG, (E), FinNone>;
+  switch (epi) {
+    QCU_CASE(0)
+    QCU_CASE(EPI_CPRE)
+    QCU_CASE(EPI_XPAY)
+    QCU_CASE(EPI_XPAY | EPI_CX)
+    QCU_CASE(EPI_XPAY | EPI_CPOST)
+    QCU_CASE(EPI_CPRE | EPI_XPAY)
+    QCU_CASE(EPI_CPRE | EPI_XPAY | EPI_NORM)
+    QCU_CASE(EPI_CPRE | EPI_XPAY | EPI_OUT2)
+    QCU_CASE(EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM)
+    QCU_CASE(EPI_XPAY | EPI_NORM)
+    default:
+      return nullptr;
+  }
+#undef QCU_CASE
+}
+
+}  // namespace qcu

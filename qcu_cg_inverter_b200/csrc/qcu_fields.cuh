@@ -1,0 +1,372 @@
+// Loads and stores of spinors, links and packed clover blocks in the internal
+// site-blocked SoA layout (chunk_index in qcu_common.cuh), for the three
+// storage precisions. Arithmetic is double for PREC_DOUBLE and float otherwise.
+#pragma once
+#include "qcu_common.cuh"
+
+namespace qcu {
+
+// A view of one spinor field (one parity, nrhs right-hand sides).
+struct SpinorView {
+  void* data;
+  float* norm;  // PREC_HALF only: one norm per (site, rhs), index s*nrhs + r
+  int nrhs;
+};
+struct CSpinorView {
+  const void* data;
+  const float* norm;
+  int nrhs;
+  CSpinorView() = default;
+  QCU_HD CSpinorView(const void* d, const float* n, int r) : data(d), norm(n), nrhs(r) {}
+  QCU_HD CSpinorView(const SpinorView& v) : data(v.data), norm(v.norm), nrhs(v.nrhs) {}
+};
+
+// ---------------- spinors ----------------
+template <int P> struct SpinorIO;
+
+template <> struct SpinorIO<PREC_DOUBLE> {
+  typedef double R;
+  static QCU_D void load(Spinor<R>& v, const CSpinorView& f, int s, int r) {
+    const double2* p = static_cast<const double2*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      double2 w = p[chunk_index(c, s, r, 12, f.nrhs)];
+      v.c[c] = mk(w.x, w.y);
+    }
+  }
+  static QCU_D void store(const SpinorView& f, int s, int r, const Spinor<R>& v) {
+    double2* p = static_cast<double2*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 12; c++) p[chunk_index(c, s, r, 12, f.nrhs)] = make_double2(v.c[c].re, v.c[c].im);
+  }
+};
+
+template <> struct SpinorIO<PREC_SINGLE> {
+  typedef float R;
+  static QCU_D void load(Spinor<R>& v, const CSpinorView& f, int s, int r) {
+    const float4* p = static_cast<const float4*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      float4 w = p[chunk_index(c, s, r, 6, f.nrhs)];
+      v.c[2 * c] = mk(w.x, w.y);
+      v.c[2 * c + 1] = mk(w.z, w.w);
+    }
+  }
+  static QCU_D void store(const SpinorView& f, int s, int r, const Spinor<R>& v) {
+    float4* p = static_cast<float4*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      p[chunk_index(c, s, r, 6, f.nrhs)] = make_float4(v.c[2 * c].re, v.c[2 * c].im, v.c[2 * c + 1].re, v.c[2 * c + 1].im);
+  }
+};
+
+QCU_D float lo16(int w) { return (float)(short)(w & 0xffff); }
+QCU_D float hi16(int w) { return (float)(short)(w >> 16); }
+QCU_D int pack16(float a, float b) {
+  return (__float2int_rn(a) & 0xffff) | (__float2int_rn(b) << 16);
+}
+
+template <> struct SpinorIO<PREC_HALF> {
+  typedef float R;
+  static QCU_D void load(Spinor<R>& v, const CSpinorView& f, int s, int r) {
+    const int4* p = static_cast<const int4*>(f.data);
+    float nm = f.norm[(size_t)s * f.nrhs + r] * kInvFix;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int4 w = p[chunk_index(c, s, r, 3, f.nrhs)];
+      v.c[4 * c + 0] = mk(lo16(w.x) * nm, hi16(w.x) * nm);
+      v.c[4 * c + 1] = mk(lo16(w.y) * nm, hi16(w.y) * nm);
+      v.c[4 * c + 2] = mk(lo16(w.z) * nm, hi16(w.z) * nm);
+      v.c[4 * c + 3] = mk(lo16(w.w) * nm, hi16(w.w) * nm);
+    }
+  }
+  static QCU_D void store(const SpinorView& f, int s, int r, const Spinor<R>& v) {
+    float mx = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) mx = fmaxf(mx, fmaxf(fabsf(v.c[k].re), fabsf(v.c[k].im)));
+    float sc = mx > 0.f ? kFix / mx : 0.f;
+    int4* p = static_cast<int4*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int4 w;
+      w.x = pack16(v.c[4 * c + 0].re * sc, v.c[4 * c + 0].im * sc);
+      w.y = pack16(v.c[4 * c + 1].re * sc, v.c[4 * c + 1].im * sc);
+      w.z = pack16(v.c[4 * c + 2].re * sc, v.c[4 * c + 2].im * sc);
+      w.w = pack16(v.c[4 * c + 3].re * sc, v.c[4 * c + 3].im * sc);
+      p[chunk_index(c, s, r, 3, f.nrhs)] = w;
+    }
+    f.norm[(size_t)s * f.nrhs + r] = mx;
+  }
+};
+
+// ---------------- links ----------------
+// gauge field: [dir][parity] sub-arrays of Vh_pad sites each
+template <int P> struct LinkIO;
+
+template <> struct LinkIO<PREC_DOUBLE> {
+  typedef double R;
+  static QCU_D void load(Link<R>& L, const void* gauge, int Vh_pad, int mu, int parity, int s) {
+    const double2* p = static_cast<const double2*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 6;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      double2 w = __ldg(p + chunk_index(c, s, 0, 6, 1));
+      L.u[c] = mk(w.x, w.y);
+    }
+    su3_reconstruct(L);
+  }
+  static QCU_D void store(void* gauge, int Vh_pad, int mu, int parity, int s, const Link<R>& L) {
+    double2* p = static_cast<double2*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 6;
+#pragma unroll
+    for (int c = 0; c < 6; c++) p[chunk_index(c, s, 0, 6, 1)] = make_double2(L.u[c].re, L.u[c].im);
+  }
+};
+
+template <> struct LinkIO<PREC_SINGLE> {
+  typedef float R;
+  static QCU_D void load(Link<R>& L, const void* gauge, int Vh_pad, int mu, int parity, int s) {
+    const float4* p = static_cast<const float4*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 3;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float4 w = __ldg(p + chunk_index(c, s, 0, 3, 1));
+      L.u[2 * c] = mk(w.x, w.y);
+      L.u[2 * c + 1] = mk(w.z, w.w);
+    }
+    su3_reconstruct(L);
+  }
+  template <class RS>
+  static QCU_D void store(void* gauge, int Vh_pad, int mu, int parity, int s, const Link<RS>& L) {
+    float4* p = static_cast<float4*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 3;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      p[chunk_index(c, s, 0, 3, 1)] = make_float4((float)L.u[2 * c].re, (float)L.u[2 * c].im,
+                                                  (float)L.u[2 * c + 1].re, (float)L.u[2 * c + 1].im);
+  }
+};
+
+template <> struct LinkIO<PREC_HALF> {
+  typedef float R;
+  static QCU_D void load(Link<R>& L, const void* gauge, int Vh_pad, int mu, int parity, int s) {
+    const int2* p = static_cast<const int2*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 3;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int2 w = __ldg(p + chunk_index(c, s, 0, 3, 1));
+      L.u[2 * c] = mk(lo16(w.x) * kInvFix, hi16(w.x) * kInvFix);
+      L.u[2 * c + 1] = mk(lo16(w.y) * kInvFix, hi16(w.y) * kInvFix);
+    }
+    su3_reconstruct(L);
+  }
+  template <class RS>
+  static QCU_D void store(void* gauge, int Vh_pad, int mu, int parity, int s, const Link<RS>& L) {
+    int2* p = static_cast<int2*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 3;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int2 w;
+      w.x = pack16((float)L.u[2 * c].re * kFix, (float)L.u[2 * c].im * kFix);
+      w.y = pack16((float)L.u[2 * c + 1].re * kFix, (float)L.u[2 * c + 1].im * kFix);
+      p[chunk_index(c, s, 0, 3, 1)] = w;
+    }
+  }
+};
+
+// ---------------- packed clover ----------------
+// One Hermitian 6x6 block: d[6] real diagonal, o[15] strictly-lower entries
+// (row i > column j at tri_index(i,j)).
+template <class R> struct HermBlock {
+  R d[6];
+  Cplx<R> o[15];
+};
+
+// v <- B v for one block
+template <class R> QCU_D void herm_apply(const HermBlock<R>& B, Cplx<R> v[6]) {
+  Cplx<R> o[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) o[i] = B.d[i] * v[i];
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      cmac(o[i], B.o[tri_index(i, j)], v[j]);
+      cmac_conj(o[j], B.o[tri_index(i, j)], v[i]);
+    }
+#pragma unroll
+  for (int i = 0; i < 6; i++) v[i] = o[i];
+}
+
+template <int P> struct CloverIO;
+
+// clover field: [parity] sub-arrays of Vh_pad sites each; clover_index picks a
+// whole field (several kappa*c_sw values can be resident side by side).
+template <> struct CloverIO<PREC_DOUBLE> {
+  typedef double R;
+  static QCU_D void load_block(HermBlock<R>& B, const void* clov, int Vh_pad, int parity, int s, int b) {
+    const double2* p = static_cast<const double2*>(clov) + (size_t)parity * Vh_pad * 36;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      double2 w = __ldg(p + chunk_index(b * 18 + k, s, 0, 36, 1));
+      B.d[2 * k] = w.x;
+      B.d[2 * k + 1] = w.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 15; k++) {
+      double2 w = __ldg(p + chunk_index(b * 18 + 3 + k, s, 0, 36, 1));
+      B.o[k] = mk(w.x, w.y);
+    }
+  }
+  template <class RS>
+  static QCU_D void store_block(void* clov, int Vh_pad, int parity, int s, int b, const HermBlock<RS>& B, float*) {
+    double2* p = static_cast<double2*>(clov) + (size_t)parity * Vh_pad * 36;
+#pragma unroll
+    for (int k = 0; k < 3; k++) p[chunk_index(b * 18 + k, s, 0, 36, 1)] = make_double2(B.d[2 * k], B.d[2 * k + 1]);
+#pragma unroll
+    for (int k = 0; k < 15; k++) p[chunk_index(b * 18 + 3 + k, s, 0, 36, 1)] = make_double2(B.o[k].re, B.o[k].im);
+  }
+};
+
+// single and half: the 36 reals of block b are reals [36b, 36b+36) of the
+// site's 72, in the order d0..d5, o0.re, o0.im, ..., o14.re, o14.im
+template <> struct CloverIO<PREC_SINGLE> {
+  typedef float R;
+  static QCU_D void load_block(HermBlock<R>& B, const void* clov, int Vh_pad, int parity, int s, int b) {
+    const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
+    float a[36];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float4 w = __ldg(p + chunk_index(b * 9 + k, s, 0, 18, 1));
+      a[4 * k] = w.x; a[4 * k + 1] = w.y; a[4 * k + 2] = w.z; a[4 * k + 3] = w.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) B.d[k] = a[k];
+#pragma unroll
+    for (int k = 0; k < 15; k++) B.o[k] = mk(a[6 + 2 * k], a[7 + 2 * k]);
+  }
+  template <class RS>
+  static QCU_D void store_block(void* clov, int Vh_pad, int parity, int s, int b, const HermBlock<RS>& B, float*) {
+    float4* p = static_cast<float4*>(clov) + (size_t)parity * Vh_pad * 18;
+    float a[36];
+#pragma unroll
+    for (int k = 0; k < 6; k++) a[k] = (float)B.d[k];
+#pragma unroll
+    for (int k = 0; k < 15; k++) { a[6 + 2 * k] = (float)B.o[k].re; a[7 + 2 * k] = (float)B.o[k].im; }
+#pragma unroll
+    for (int k = 0; k < 9; k++) p[chunk_index(b * 9 + k, s, 0, 18, 1)] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+  }
+};
+
+template <> struct CloverIO<PREC_HALF> {
+  typedef float R;
+  // 72 int16 per site = 9 int4 chunks; the norm array ([parity][Vh_pad] floats)
+  // follows the chunk array of both parities.
+  static QCU_D const float* norms(const void* clov, int Vh_pad) {
+    return reinterpret_cast<const float*>(static_cast<const int4*>(clov) + (size_t)2 * Vh_pad * 9);
+  }
+  static QCU_D int word(const int4* w, int k) {
+    const int4 c = w[k >> 2];
+    int l = k & 3;
+    return l == 0 ? c.x : (l == 1 ? c.y : (l == 2 ? c.z : c.w));
+  }
+  static QCU_D void decode(HermBlock<R>& B, const int4 w[9], int b, float nm) {
+    float a[36];
+#pragma unroll
+    for (int k = 0; k < 18; k++) {
+      int v = word(w, b * 18 + k);
+      a[2 * k] = lo16(v) * nm;
+      a[2 * k + 1] = hi16(v) * nm;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) B.d[k] = a[k];
+#pragma unroll
+    for (int k = 0; k < 15; k++) B.o[k] = mk(a[6 + 2 * k], a[7 + 2 * k]);
+  }
+  static QCU_D void load_block(HermBlock<R>& B, const void* clov, int Vh_pad, int parity, int s, int b) {
+    const int4* p = static_cast<const int4*>(clov) + (size_t)parity * Vh_pad * 9;
+    int4 w[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) w[c] = __ldg(p + chunk_index(c, s, 0, 9, 1));
+    float nm = __ldg(norms(clov, Vh_pad) + (size_t)parity * Vh_pad + s) * kInvFix;
+    decode(B, w, b, nm);
+  }
+  // stores both blocks; the site norm is the largest |real| over both
+  template <class RS>
+  static QCU_D void store_site(void* clov, int Vh_pad, int parity, int s, const HermBlock<RS> B[2]) {
+    float mx = 0.f;
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) mx = fmaxf(mx, fabsf((float)B[b].d[k]));
+#pragma unroll
+      for (int k = 0; k < 15; k++) mx = fmaxf(mx, fmaxf(fabsf((float)B[b].o[k].re), fabsf((float)B[b].o[k].im)));
+    }
+    float sc = mx > 0.f ? kFix / mx : 0.f;
+    int words[36];
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) words[b * 18 + k] = pack16((float)B[b].d[2 * k] * sc, (float)B[b].d[2 * k + 1] * sc);
+#pragma unroll
+      for (int k = 0; k < 15; k++) words[b * 18 + 3 + k] = pack16((float)B[b].o[k].re * sc, (float)B[b].o[k].im * sc);
+    }
+    int4* p = static_cast<int4*>(clov) + (size_t)parity * Vh_pad * 9;
+#pragma unroll
+    for (int c = 0; c < 9; c++) p[chunk_index(c, s, 0, 9, 1)] = make_int4(words[4 * c], words[4 * c + 1], words[4 * c + 2], words[4 * c + 3]);
+    float* nrm = const_cast<float*>(norms(clov, Vh_pad));
+    nrm[(size_t)parity * Vh_pad + s] = mx;
+  }
+};
+
+// v <- blockdiag(B0, B1) v with the site's packed clover (one block at a time
+// for double/single; the 16-bit form is fetched in one go, 9 x 16 bytes).
+template <int P, class R>
+QCU_D void clover_apply_site(Spinor<R>& v, const void* clov, int Vh_pad, int parity, int s) {
+  if constexpr (P == PREC_HALF) {
+    const int4* p = static_cast<const int4*>(clov) + (size_t)parity * Vh_pad * 9;
+    int4 w[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) w[c] = __ldg(p + chunk_index(c, s, 0, 9, 1));
+    float nm = __ldg(CloverIO<PREC_HALF>::norms(clov, Vh_pad) + (size_t)parity * Vh_pad + s) * kInvFix;
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      HermBlock<float> B;
+      CloverIO<PREC_HALF>::decode(B, w, b, nm);
+      Cplx<float> t[6];
+#pragma unroll
+      for (int i = 0; i < 6; i++) t[i] = mk((float)v.c[6 * b + i].re, (float)v.c[6 * b + i].im);
+      herm_apply(B, t);
+#pragma unroll
+      for (int i = 0; i < 6; i++) v.c[6 * b + i] = mk((R)t[i].re, (R)t[i].im);
+    }
+  } else {
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      HermBlock<typename CloverIO<P>::R> B;
+      CloverIO<P>::load_block(B, clov, Vh_pad, parity, s, b);
+      Cplx<typename CloverIO<P>::R> t[6];
+#pragma unroll
+      for (int i = 0; i < 6; i++) t[i] = mk((typename CloverIO<P>::R)v.c[6 * b + i].re, (typename CloverIO<P>::R)v.c[6 * b + i].im);
+      herm_apply(B, t);
+#pragma unroll
+      for (int i = 0; i < 6; i++) v.c[6 * b + i] = mk((R)t[i].re, (R)t[i].im);
+    }
+  }
+}
+
+// bytes of a clover field (both parities) in the given precision
+inline size_t clover_field_bytes(int P, int Vh_pad) {
+  if (P == PREC_DOUBLE) return (size_t)2 * Vh_pad * 36 * 16;
+  if (P == PREC_SINGLE) return (size_t)2 * Vh_pad * 18 * 16;
+  return (size_t)2 * Vh_pad * 9 * 16 + (size_t)2 * Vh_pad * 4;
+}
+inline size_t gauge_field_bytes(int P, int Vh_pad) {
+  if (P == PREC_DOUBLE) return (size_t)8 * Vh_pad * 6 * 16;
+  if (P == PREC_SINGLE) return (size_t)8 * Vh_pad * 3 * 16;
+  return (size_t)8 * Vh_pad * 3 * 8;
+}
+inline size_t spinor_field_bytes(int P, int Vh_pad, int nrhs) {
+  if (P == PREC_DOUBLE) return (size_t)Vh_pad * nrhs * 12 * 16;
+  if (P == PREC_SINGLE) return (size_t)Vh_pad * nrhs * 6 * 16;
+  return (size_t)Vh_pad * nrhs * 3 * 16;
+}
+inline size_t spinor_norm_bytes(int P, int Vh_pad, int nrhs) {
+  return P == PREC_HALF ? (size_t)Vh_pad * nrhs * 4 : 0;
+}
+
+}  // namespace qcu

@@ -1,0 +1,60 @@
+// Kernel argument structs and host launchers shared by the library's .cu files.
+#pragma once
+#include "qcu_common.cuh"
+#include "qcu_fields.cuh"
+#include "qcu_reduce.cuh"
+
+namespace qcu {
+
+// Epilogue flags of the fused stencil kernel. With h = D^(dag) in (the hop),
+// C the clover field of the output parity, a the per-RHS coefficient and x the
+// xpay input, the output is
+//   EPI_CPRE           : out = C h
+//   EPI_XPAY           : out = x + a h           (with EPI_CPRE: x + a C h)
+//   EPI_XPAY|EPI_CX    : out = C x + a h
+//   EPI_CPOST          : out = C (x + a h)       (needs EPI_XPAY)
+//   EPI_OUT2           : also out2 = C out
+//   EPI_NORM           : reduce |out|^2 per RHS (finishing functor FinId)
+enum EpiFlags : int {
+  EPI_CPRE = 1,
+  EPI_XPAY = 2,
+  EPI_CX = 4,
+  EPI_CPOST = 8,
+  EPI_OUT2 = 16,
+  EPI_NORM = 32,
+};
+
+struct DslashArgs {
+  Geom g;
+  int parity;            // parity of the output sites
+  int nrhs;
+  CSpinorView in;        // parity 1-parity
+  SpinorView out;
+  CSpinorView x;         // xpay input, output parity
+  SpinorView out2;
+  const void* gauge;
+  const void* clover;    // clover (or its inverse) field 0, both parities
+  size_t clover_stride;  // bytes between resident clover fields
+  const int* clover_idx; // per-RHS field index, nullptr -> field 0
+  const double* coef;    // per-RHS a, nullptr -> coef0
+  double coef0;
+  double bc_t;
+  const int* active;     // per-RHS mask, nullptr -> all active
+  ReduceArgs red;
+};
+
+// Finishing functors available to fused reductions (see solver kernels).
+enum FinId : int { FIN_NONE = 0, FIN_CG_ALPHA = 1, FIN_CG_BETA = 2 };
+
+// Launch configuration: block = (Rb rhs lanes, Sb site lanes).
+struct LaunchShape {
+  int Rb, Sb;
+};
+
+cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape shape,
+                          cudaStream_t stream);
+
+// Number of blocks along x for a field of Vh sites.
+inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }
+
+}  // namespace qcu

@@ -1,0 +1,85 @@
+// Deterministic single-pass reductions.
+//
+// Kernels run with a 2-D thread block: threadIdx.x = right-hand side within the
+// block's RHS tile (Rb lanes), threadIdx.y = site. Each block reduces its
+// per-RHS values with warp shuffles (over the site lanes only) and shared
+// memory, writes one partial per (rhs, quantity), and the last block to finish
+// (atomic ticket) sums the partials in a fixed order and calls a finishing
+// functor with the totals. The result therefore depends only on the launch
+// shape, never on timing. Partials and tickets live in caller-provided scratch
+// memory; the last block re-arms the ticket to 0.
+#pragma once
+#include "qcu_common.cuh"
+
+namespace qcu {
+
+struct ReduceArgs {
+  double* partial;      // [nrhs*NR][gridDim.x] doubles
+  unsigned* ticket;     // one counter, 0 on entry
+  double* result;       // [nrhs*NR] totals (written by the last block)
+  void* state;          // passed to the finishing functor
+};
+
+// No finishing step: totals are left in result[].
+struct FinNone {
+  static QCU_D void apply(const double*, int, int, void*) {}
+};
+
+constexpr int kMaxWarps = 32;
+
+// vals: NR values of this thread (zero for idle threads). Every thread of the
+// block must call this.
+template <int NR, class Fin>
+QCU_D void block_reduce_finish(double vals[NR], int nrhs, const ReduceArgs& red) {
+  __shared__ double sm[kMaxWarps][NR * 32];
+  __shared__ bool am_last;
+  const int Rb = blockDim.x;
+  const int tid = threadIdx.y * Rb + threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int nthreads = Rb * blockDim.y;
+  const int nwarps = (nthreads + 31) >> 5;
+  // reduce over the site lanes of the warp (lanes that share threadIdx.x)
+#pragma unroll
+  for (int k = 0; k < NR; k++)
+    for (int off = 16; off >= Rb; off >>= 1) vals[k] += __shfl_xor_sync(0xffffffffu, vals[k], off);
+  if (lane < Rb)
+    for (int k = 0; k < NR; k++) sm[warp][k * 32 + lane] = vals[k];
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    int r = blockIdx.y * Rb + threadIdx.x;
+    if (r < nrhs) {
+      for (int k = 0; k < NR; k++) {
+        double acc = 0.0;
+        for (int w = 0; w < nwarps; w++) acc += sm[w][k * 32 + threadIdx.x];
+        red.partial[(size_t)(r * NR + k) * gridDim.x + blockIdx.x] = acc;
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    unsigned total = gridDim.x * gridDim.y;
+    unsigned t = atomicAdd(red.ticket, 1u);
+    am_last = (t == total - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  // last block: one warp per (rhs, quantity), lanes stride over the blocks
+  const int nq = nrhs * NR;
+  for (int q = warp; q < nq; q += nwarps) {
+    double acc = 0.0;
+    const volatile double* p = red.partial + (size_t)q * gridDim.x;
+    for (int b = lane; b < (int)gridDim.x; b += 32) acc += p[b];
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) red.result[q] = acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    Fin::apply(red.result, nrhs, NR, red.state);
+    __threadfence();
+    *red.ticket = 0u;
+  }
+}
+
+}  // namespace qcu

@@ -1,0 +1,531 @@
+// Even-odd preconditioned CG for M = A - kappa*D with mixed precision and
+// reliable updates, batched over right-hand sides (each RHS with its own
+// kappa, CG scalars and stopping point).
+//
+// Schur system on the even sites (the reference solves the full lattice with
+// a non-Hermitian pseudo-normal operator, src/cg_inverter.cu:260-369 and
+// src/qcu_clover_dslash.cu:1044-1049; this is the mathematically consistent
+// replacement, with the true adjoint):
+//   Mhat      = 1 - kappa^2 A_ee^-1 D_eo A_oo^-1 D_oe
+//   Mhat^dag  = 1 - kappa^2 D^dag_eo A_oo^-1 D^dag_oe A_ee^-1
+//   bhat      = A_ee^-1 (b_e + kappa D_eo A_oo^-1 b_o)
+//   CG on Mhat^dag Mhat x_e = Mhat^dag bhat, then
+//   x_o       = A_oo^-1 (b_o + kappa D_oe x_e).
+// The full-system residual of that x is exactly A_ee (bhat - Mhat x_e) on the
+// even sites and zero on the odd ones, so every reliable update measures the
+// true residual |b - M x| / |b| in FP64 and the solve stops on it.
+//
+// Inner iterations run in the sloppy precision (16-bit or single storage,
+// FP32 arithmetic; or FP64), six fused kernels per iteration, all scalars
+// on the device. Chunks of iterations are replayed as CUDA graphs; the host
+// looks at the per-RHS state once per chunk.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "qcu_context.h"
+
+namespace qcu {
+
+enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_RES_R2, D_RES_AR2, D_RES_NE, D_BNORM, D_NUM };
+enum { I_ACTIVE = 0, I_EVENT, I_ITERS, I_BREAK, I_CIDX, I_UPD, I_ALL, I_NUM };
+
+struct SolverWorkspace {
+  int nrhs = 0, ps = -1, pa = -1;
+  int vh_pad = 0;
+  bool clover = false;
+  Field b2, bh, xhi, t64, y64, u64, z64, xo;
+  Field xlo, rlo, p, t, y, u, z;
+  DevBuf mem;       // [D_NUM][nrhs] doubles then [I_NUM][nrhs] ints
+  DevBuf dstate;    // CgDevState on the device
+  PinnedBuf hmem;   // host mirror of mem
+  CgDevState st;
+  LaunchShape shape{1, 128};
+  std::vector<std::pair<int, cudaGraphExec_t>> graphs;
+  ~SolverWorkspace() { drop_graphs(); }
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+  }
+  double* dd(int k) const { return mem.as<double>() + (size_t)k * nrhs; }
+  int* di(int k) const { return reinterpret_cast<int*>(mem.as<double>() + (size_t)D_NUM * nrhs) + (size_t)k * nrhs; }
+  double* hd(int k) const { return hmem.as<double>() + (size_t)k * nrhs; }
+  int* hi(int k) const { return reinterpret_cast<int*>(hmem.as<double>() + (size_t)D_NUM * nrhs) + (size_t)k * nrhs; }
+  size_t mem_bytes() const { return (size_t)D_NUM * nrhs * sizeof(double) + (size_t)I_NUM * nrhs * sizeof(int); }
+};
+
+static LaunchShape shape_for(int nrhs) {
+  if (nrhs <= 1) return LaunchShape{1, 128};
+  int rb = 1;
+  while (rb * 2 <= nrhs && rb * 2 <= 8) rb *= 2;
+  return LaunchShape{rb, 128 / rb};
+}
+
+static int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover) {
+  cudaStream_t st = ctx->stream;
+  const int pa = (ps == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  const int vp = ctx->g.Vh_pad;
+  if (w.nrhs != nrhs || w.ps != ps || w.vh_pad != vp) w.drop_graphs();
+  w.clover = clover;
+  w.shape = shape_for(nrhs);
+  QCU_CHECK(w.b2.alloc(PREC_DOUBLE, vp, nrhs, 2, st));
+  for (Field* f : {&w.bh, &w.xhi, &w.t64, &w.y64, &w.u64, &w.z64, &w.xo}) QCU_CHECK(f->alloc(PREC_DOUBLE, vp, nrhs, 1, st));
+  QCU_CHECK(w.xlo.alloc(pa, vp, nrhs, 1, st));
+  QCU_CHECK(w.rlo.alloc(pa, vp, nrhs, 1, st));
+  for (Field* f : {&w.p, &w.t, &w.y, &w.u, &w.z}) QCU_CHECK(f->alloc(ps, vp, nrhs, 1, st));
+  if (w.nrhs != nrhs || !w.mem.p) {
+    w.nrhs = nrhs;
+    w.mem.release();
+    QCU_CHECK(w.mem.ensure(w.mem_bytes(), st));
+    QCU_CHECK(w.hmem.ensure(w.mem_bytes()));
+    QCU_CHECK(w.dstate.ensure(sizeof(CgDevState), st));
+  }
+  w.nrhs = nrhs;
+  w.ps = ps;
+  w.pa = pa;
+  w.vh_pad = vp;
+  w.st.rr = w.dd(D_RR);
+  w.st.rr_old = w.dd(D_RROLD);
+  w.st.pAp = w.dd(D_PAP);
+  w.st.alpha = w.dd(D_ALPHA);
+  w.st.beta = w.dd(D_BETA);
+  w.st.trigger = w.dd(D_TRIG);
+  w.st.active = w.di(I_ACTIVE);
+  w.st.event = w.di(I_EVENT);
+  w.st.iters = w.di(I_ITERS);
+  w.st.breakdown = w.di(I_BREAK);
+  QCU_CHECK_CUDA(cudaMemcpyAsync(w.dstate.p, &w.st, sizeof(CgDevState), cudaMemcpyHostToDevice, st));
+  QCU_CHECK(ctx->red.ensure(ctx->g, nrhs, st));
+  return QCU_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// building blocks
+// ---------------------------------------------------------------------------
+struct OpCtx {
+  qcu_context ctx;
+  SolverWorkspace* w;
+  double bc_t;
+  cudaStream_t st;
+};
+
+static DslashArgs op_args(const OpCtx& o, int prec, int parity, const Field& in, const Field& out, const int* mask) {
+  DslashArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = o.ctx->g;
+  a.parity = parity;
+  a.nrhs = o.w->nrhs;
+  a.in = in.cview(0);
+  a.out = out.view(0);
+  a.gauge = ctx_gauge(o.ctx, prec);
+  a.clover = ctx_clover_ptr(o.ctx, prec, true);
+  a.clover_stride = ctx_clover_stride(o.ctx, prec);
+  a.clover_idx = o.w->di(I_CIDX);
+  a.bc_t = o.bc_t;
+  a.active = mask;
+  return a;
+}
+
+static int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& a) {
+  QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, fin, a, o.w->shape, o.st));
+  o.ctx->launches++;
+  return QCU_SUCCESS;
+}
+
+static ReduceArgs red_into(const OpCtx& o, double* result, bool with_state) {
+  ReduceArgs r = o.ctx->red.args(with_state ? o.w->dstate.p : nullptr);
+  r.result = result;
+  return r;
+}
+
+// One sloppy CG iteration (six launches), masked by the active flags.
+static int sloppy_iteration(const OpCtx& o) {
+  SolverWorkspace& w = *o.w;
+  const int ps = w.ps;
+  const int* act = w.st.active;
+  // t = A_oo^-1 D_oe p
+  {
+    DslashArgs a = op_args(o, ps, 1, w.p, w.t, act);
+    QCU_CHECK(dsl(o, ps, false, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  }
+  // y = p - k^2 A_ee^-1 D_eo t, u = A_ee^-1 y, pAp = |y|^2 -> alpha
+  {
+    DslashArgs a = op_args(o, ps, 0, w.t, w.y, act);
+    a.x = w.p.cview(0);
+    a.out2 = w.u.view(0);
+    a.coef = w.dd(D_MK2);
+    a.red = red_into(o, o.ctx->red.result.as<double>(), true);
+    int epi = w.clover ? (EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM) : (EPI_XPAY | EPI_NORM);
+    QCU_CHECK(dsl(o, ps, false, epi, FIN_CG_ALPHA, a));
+  }
+  // t = A_oo^-1 D^dag_oe u
+  {
+    DslashArgs a = op_args(o, ps, 1, w.clover ? w.u : w.y, w.t, act);
+    QCU_CHECK(dsl(o, ps, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  }
+  // z = y - k^2 D^dag_eo t
+  {
+    DslashArgs a = op_args(o, ps, 0, w.t, w.z, act);
+    a.x = w.y.cview(0);
+    a.coef = w.dd(D_MK2);
+    QCU_CHECK(dsl(o, ps, true, EPI_XPAY, FIN_NONE, a));
+  }
+  // x += alpha p, r -= alpha z, rr -> beta
+  QCU_CHECK_CUDA(launch_cg_xr(w.pa, ps, o.ctx->g.Vh, w.nrhs, w.xlo.view(0), w.rlo.view(0), w.p.cview(0), w.z.cview(0),
+                              w.st.alpha, act, red_into(o, o.ctx->red.result.as<double>(), true), w.shape, o.st));
+  // p = r + beta p
+  QCU_CHECK_CUDA(launch_cg_p(w.pa, ps, o.ctx->g.Vh, w.nrhs, w.p.view(0), w.rlo.cview(0), w.st.beta, act, w.shape, o.st));
+  o.ctx->launches += 2;
+  return QCU_SUCCESS;
+}
+
+// FP64 true residual for the RHS in mask `upd`: x_hi += x_lo, r = bhat - Mhat
+// x_hi, |r|^2, |A_ee r|^2 (the full-system residual), r_ne = Mhat^dag r and
+// |r_ne|^2 (into D_RES_R2, D_RES_AR2, D_RES_NE).
+static int reliable_update(const OpCtx& o) {
+  SolverWorkspace& w = *o.w;
+  const int* upd = w.di(I_UPD);
+  const int Vh = o.ctx->g.Vh;
+  QCU_CHECK_CUDA(launch_accumulate(w.pa, Vh, w.nrhs, w.xhi.view(0), w.xlo.view(0), upd, w.shape, o.st));
+  o.ctx->launches++;
+  {
+    DslashArgs a = op_args(o, PREC_DOUBLE, 1, w.xhi, w.t64, upd);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  }
+  {
+    DslashArgs a = op_args(o, PREC_DOUBLE, 0, w.t64, w.y64, upd);
+    a.x = w.xhi.cview(0);
+    a.coef = w.dd(D_MK2);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? (EPI_CPRE | EPI_XPAY) : EPI_XPAY, FIN_NONE, a));
+  }
+  // r = bhat - Mhat x (in y64)
+  QCU_CHECK_CUDA(launch_residual(Vh, w.nrhs, w.y64.view(0), w.bh.cview(0), w.y64.cview(0), upd,
+                                 red_into(o, w.dd(D_RES_R2), false), w.shape, o.st));
+  o.ctx->launches++;
+  if (w.clover) {
+    ReduceArgs ra = red_into(o, w.dd(D_RES_AR2), false);
+    SpinorView none{nullptr, nullptr, w.nrhs};
+    QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0), none,
+                                       ctx_clover_ptr(o.ctx, PREC_DOUBLE, false), ctx_clover_stride(o.ctx, PREC_DOUBLE),
+                                       w.di(I_CIDX), upd, &ra, w.shape, o.st));
+    QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0), w.u64.view(0),
+                                       ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
+                                       w.di(I_CIDX), upd, nullptr, w.shape, o.st));
+    o.ctx->launches += 2;
+  }
+  {
+    DslashArgs a = op_args(o, PREC_DOUBLE, 1, w.clover ? w.u64 : w.y64, w.t64, upd);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  }
+  {
+    DslashArgs a = op_args(o, PREC_DOUBLE, 0, w.t64, w.z64, upd);
+    a.x = w.y64.cview(0);
+    a.coef = w.dd(D_MK2);
+    a.red = red_into(o, w.dd(D_RES_NE), false);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, true, EPI_XPAY | EPI_NORM, FIN_NONE, a));
+  }
+  return QCU_SUCCESS;
+}
+
+static int pull_state(const OpCtx& o) {
+  SolverWorkspace& w = *o.w;
+  QCU_CHECK_CUDA(cudaMemcpyAsync(w.hmem.p, w.mem.p, w.mem_bytes(), cudaMemcpyDeviceToHost, o.st));
+  QCU_CHECK_CUDA(cudaStreamSynchronize(o.st));
+  return QCU_SUCCESS;
+}
+// The host mirror is edited right after a push, so the copy must have left
+// the pinned buffer before this returns.
+static int push_state(const OpCtx& o) {
+  SolverWorkspace& w = *o.w;
+  QCU_CHECK_CUDA(cudaMemcpyAsync(w.mem.p, w.hmem.p, w.mem_bytes(), cudaMemcpyHostToDevice, o.st));
+  QCU_CHECK_CUDA(cudaStreamSynchronize(o.st));
+  return QCU_SUCCESS;
+}
+
+static int run_chunk(const OpCtx& o, int K, bool graphs) {
+  SolverWorkspace& w = *o.w;
+  if (!graphs) {
+    for (int k = 0; k < K; k++) QCU_CHECK(sloppy_iteration(o));
+    return QCU_SUCCESS;
+  }
+  cudaGraphExec_t exec = nullptr;
+  for (auto& g : w.graphs)
+    if (g.first == K) exec = g.second;
+  if (!exec) {
+    long long before = o.ctx->launches;
+    QCU_CHECK_CUDA(cudaStreamBeginCapture(o.st, cudaStreamCaptureModeThreadLocal));
+    int s = QCU_SUCCESS;
+    for (int k = 0; k < K && s == QCU_SUCCESS; k++) s = sloppy_iteration(o);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(o.st, &graph);
+    if (s != QCU_SUCCESS) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
+    }
+    QCU_CHECK_CUDA(e);
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    QCU_CHECK_CUDA(e);
+    w.graphs.push_back({K, exec});
+    o.ctx->launches = before;  // captured launches are counted when replayed
+  }
+  QCU_CHECK_CUDA(cudaGraphLaunch(exec, o.st));
+  o.ctx->launches += 6LL * K;
+  return QCU_SUCCESS;
+}
+
+}  // namespace qcu
+
+using namespace qcu;
+
+extern "C" void qcu_solver_workspace_free(qcu_context ctx) {
+  if (ctx) {
+    delete ctx->solver;
+    ctx->solver = nullptr;
+  }
+}
+
+extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, const double* kappas,
+                         const qcu_solve_params* params, qcu_solve_report* reports) {
+  clear_error();
+  QCU_CHECK(ctx_check(ctx));
+  if (!x || !b || nrhs < 1 || !params) {
+    set_error(QCU_ERR_INVALID_ARG, "bad solve arguments");
+    return QCU_ERR_INVALID_ARG;
+  }
+  if (!ctx->gauge_loaded) {
+    set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
+    return QCU_ERR_NOT_INITIALIZED;
+  }
+  const qcu_solve_params& P = *params;
+  if (P.precision < QCU_PREC_DOUBLE || P.precision > QCU_PREC_HALF || !(P.tol > 0) || P.maxiter < 1) {
+    set_error(QCU_ERR_INVALID_ARG, "bad solver parameters");
+    return QCU_ERR_INVALID_ARG;
+  }
+  const Geom& g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  std::vector<double> kap(nrhs);
+  for (int r = 0; r < nrhs; r++) {
+    kap[r] = kappas ? kappas[r] : P.kappa;
+    if (!(kap[r] > 0.0) || !isfinite(kap[r])) {
+      set_error(QCU_ERR_INVALID_ARG, "kappa must be positive");
+      return QCU_ERR_INVALID_ARG;
+    }
+  }
+  const bool clover = P.csw != 0.0;
+  // clover slots, one per distinct kappa*c_sw
+  std::vector<int> cidx(nrhs, 0);
+  if (clover) {
+    std::vector<double> distinct;
+    for (double k : kap)
+      if (std::find(distinct.begin(), distinct.end(), k * P.csw) == distinct.end()) distinct.push_back(k * P.csw);
+    QCU_CHECK(ctx_clover_reserve(ctx, (int)distinct.size()));
+    for (auto& pin : ctx->clover.pinned) pin = 0;
+    for (int r = 0; r < nrhs; r++) {
+      int slot;
+      QCU_CHECK(ctx_clover_slot(ctx, kap[r] * P.csw, &slot));
+      ctx->clover.pinned[slot] = 1;
+      cidx[r] = slot;
+    }
+  }
+  if (!ctx->solver) ctx->solver = new SolverWorkspace();
+  SolverWorkspace& w = *ctx->solver;
+  QCU_CHECK(ws_prepare(ctx, w, nrhs, P.precision, clover));
+  OpCtx o{ctx, &w, P.bc_t, st};
+
+  // host state
+  memset(w.hmem.p, 0, w.mem_bytes());
+  for (int r = 0; r < nrhs; r++) {
+    w.hd(D_KAPPA)[r] = kap[r];
+    w.hd(D_MK2)[r] = -kap[r] * kap[r];
+    w.hi(I_CIDX)[r] = cidx[r];
+    w.hi(I_UPD)[r] = 1;
+    w.hi(I_ALL)[r] = 1;
+  }
+  QCU_CHECK(push_state(o));
+
+  // source -> internal, |b|^2
+  const size_t full_c = (size_t)2 * g.Vh * 12;  // complex numbers of one full spinor
+  const void* bsrc = b;
+  if (!is_device_ptr(b)) {
+    QCU_CHECK(ctx->stage_in.ensure(full_c * 16 * nrhs, st));
+    QCU_CHECK_CUDA(cudaMemcpyAsync(ctx->stage_in.p, b, full_c * 16 * nrhs, cudaMemcpyHostToDevice, st));
+    bsrc = ctx->stage_in.p;
+  }
+  for (int p = 0; p < 2; p++) {
+    QCU_CHECK_CUDA(launch_spinor_in(PREC_DOUBLE, g, nrhs, static_cast<const double2*>(bsrc) + p * (full_c / 2), full_c,
+                                    w.b2.view(p), st));
+    ctx->launches++;
+  }
+  {
+    ReduceArgs ra = red_into(o, ctx->red.result.as<double>(), false);
+    QCU_CHECK_CUDA(launch_cdot(PREC_DOUBLE, 2 * g.Vh_pad, nrhs, w.b2.cview(0), w.b2.cview(0), nullptr, ra, w.shape, st));
+    ctx->launches++;
+    QCU_CHECK_CUDA(cudaMemcpyAsync(ctx->red.host.p, ctx->red.result.p, (size_t)nrhs * 2 * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    QCU_CHECK_CUDA(cudaStreamSynchronize(st));
+  }
+  std::vector<double> bnorm(nrhs);
+  for (int r = 0; r < nrhs; r++) {
+    double b2 = ctx->red.host.as<double>()[2 * r];
+    if (!isfinite(b2)) {
+      set_error(QCU_ERR_INVALID_ARG, "source contains NaN or Inf");
+      return QCU_ERR_INVALID_ARG;
+    }
+    bnorm[r] = sqrt(b2);
+  }
+  // bhat = A_ee^-1 (b_e + kappa D_eo A_oo^-1 b_o)
+  {
+    Field* bo = &w.b2;
+    DslashArgs a;
+    if (clover) {
+      QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, g, 1, nrhs, w.b2.cview(1), w.t64.view(0),
+                                         ctx_clover_ptr(ctx, PREC_DOUBLE, true), ctx_clover_stride(ctx, PREC_DOUBLE),
+                                         w.di(I_CIDX), nullptr, nullptr, w.shape, st));
+      ctx->launches++;
+      a = op_args(o, PREC_DOUBLE, 0, w.t64, w.bh, nullptr);
+    } else {
+      a = op_args(o, PREC_DOUBLE, 0, w.b2, w.bh, nullptr);
+      a.in = bo->cview(1);
+    }
+    a.x = w.b2.cview(0);
+    a.coef = w.dd(D_KAPPA);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, false, clover ? (EPI_XPAY | EPI_CPOST) : EPI_XPAY, FIN_NONE, a));
+  }
+  // x = 0 everywhere; the first "reliable update" computes r_ne = Mhat^dag bhat
+  QCU_CHECK_CUDA(cudaMemsetAsync(w.xhi.data.p, 0, w.xhi.data.bytes, st));
+  QCU_CHECK_CUDA(cudaMemsetAsync(w.xlo.data.p, 0, w.xlo.data.bytes, st));
+  QCU_CHECK_CUDA(cudaMemsetAsync(w.p.data.p, 0, w.p.data.bytes, st));
+  if (w.p.norm.p) QCU_CHECK_CUDA(cudaMemsetAsync(w.p.norm.p, 0, w.p.norm.bytes, st));
+
+  const double delta = P.delta > 0 && P.delta < 1 ? P.delta : (P.precision == QCU_PREC_DOUBLE ? 1e-2 : 0.1);
+  std::vector<int> done(nrhs, 0), conv(nrhs, 0), nupd(nrhs, 0), status(nrhs, QCU_SUCCESS);
+  std::vector<double> true_res(nrhs, 1.0), rr_at_check(nrhs, 0.0);
+  std::vector<int> it_at_check(nrhs, 0);
+  bool first = true;
+  int K = 8;
+  const bool graphs = P.use_graphs != 0;
+  for (int guard = 0; guard < 1000000; guard++) {
+    // ---- reliable updates / convergence checks for the RHS in I_UPD ----
+    bool any_upd = false;
+    for (int r = 0; r < nrhs; r++) any_upd |= w.hi(I_UPD)[r] != 0;
+    if (any_upd) {
+      QCU_CHECK(push_state(o));
+      QCU_CHECK(reliable_update(o));
+      QCU_CHECK(pull_state(o));
+      bool any_restart = false;
+      for (int r = 0; r < nrhs; r++) {
+        if (!w.hi(I_UPD)[r]) continue;
+        nupd[r]++;
+        double ar2 = clover ? w.hd(D_RES_AR2)[r] : w.hd(D_RES_R2)[r];
+        double ne2 = w.hd(D_RES_NE)[r];
+        double res = bnorm[r] > 0 ? sqrt(fmax(ar2, 0.0)) / bnorm[r] : 0.0;
+        true_res[r] = res;
+        bool stop = false;
+        if (bnorm[r] == 0.0 || res < P.tol) {
+          conv[r] = 1;
+          stop = true;
+        } else if (!isfinite(res) || w.hi(I_BREAK)[r]) {
+          status[r] = QCU_ERR_BREAKDOWN;
+          stop = true;
+        } else if (w.hi(I_ITERS)[r] >= P.maxiter) {
+          status[r] = QCU_ERR_NOT_CONVERGED;
+          stop = true;
+        }
+        if (stop) {
+          done[r] = 1;
+          w.hi(I_ACTIVE)[r] = 0;
+          w.hi(I_EVENT)[r] = 0;
+          w.hi(I_UPD)[r] = 0;
+          continue;
+        }
+        // continue: r_lo = r_ne, beta = |r_ne|^2 / rr_old, rr = |r_ne|^2
+        w.hd(D_BETA)[r] = first ? 0.0 : ne2 / w.hd(D_RROLD)[r];
+        w.hd(D_RR)[r] = ne2;
+        // next check when the iterated residual fell by delta, or earlier
+        // when the predicted true residual reaches tol
+        double q = sqrt(fmax(ar2, 1e-300) / fmax(ne2, 1e-300));
+        double target = 0.5 * P.tol * bnorm[r] / q;
+        w.hd(D_TRIG)[r] = fmax(delta * delta * ne2, target * target);
+        w.hi(I_ACTIVE)[r] = 1;
+        w.hi(I_EVENT)[r] = 0;
+        rr_at_check[r] = ne2;
+        it_at_check[r] = w.hi(I_ITERS)[r];
+        any_restart = true;
+      }
+      if (any_restart) {
+        QCU_CHECK(push_state(o));
+        // r_lo = r_ne and p = r_lo + beta p for the restarted RHS (mask I_UPD)
+        QCU_CHECK_CUDA(launch_convert(w.pa, PREC_DOUBLE, g.Vh, nrhs, w.rlo.view(0), w.z64.cview(0), w.di(I_UPD), nullptr,
+                                      w.shape, st));
+        QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, g.Vh, nrhs, w.p.view(0), w.rlo.cview(0), w.dd(D_BETA), w.di(I_UPD),
+                                   w.shape, st));
+        ctx->launches += 2;
+      }
+      for (int r = 0; r < nrhs; r++) w.hi(I_UPD)[r] = 0;
+      QCU_CHECK(push_state(o));
+      first = false;
+    }
+    bool any_active = false;
+    for (int r = 0; r < nrhs; r++) any_active |= (!done[r] && w.hi(I_ACTIVE)[r]);
+    if (!any_active) break;
+    // ---- a chunk of sloppy iterations ----
+    QCU_CHECK(run_chunk(o, K, graphs));
+    QCU_CHECK(pull_state(o));
+    // next chunk length from the observed convergence rate
+    double need = 64;
+    for (int r = 0; r < nrhs; r++) {
+      if (done[r]) continue;
+      if (w.hi(I_EVENT)[r] || w.hi(I_ITERS)[r] >= P.maxiter) w.hi(I_UPD)[r] = 1;
+      if (!w.hi(I_ACTIVE)[r]) continue;
+      int di = w.hi(I_ITERS)[r] - it_at_check[r];
+      double rr = w.hd(D_RR)[r], tr = w.hd(D_TRIG)[r];
+      if (di > 0 && rr < rr_at_check[r] && rr > tr) {
+        double rate = log(rr / rr_at_check[r]) / di;
+        need = fmin(need, log(tr / rr) / rate);
+      }
+    }
+    int k2 = 4;
+    while (k2 < 64 && k2 < need) k2 *= 2;
+    K = k2;
+  }
+  // x_e += x_lo (no-op for checked RHS), x_o = A_oo^-1 (b_o + kappa D_oe x_e)
+  for (int r = 0; r < nrhs; r++) w.hi(I_UPD)[r] = 1;
+  QCU_CHECK(push_state(o));
+  QCU_CHECK_CUDA(launch_accumulate(w.pa, g.Vh, nrhs, w.xhi.view(0), w.xlo.view(0), w.di(I_UPD), w.shape, st));
+  {
+    DslashArgs a = op_args(o, PREC_DOUBLE, 1, w.xhi, w.xo, nullptr);
+    a.x = w.b2.cview(1);
+    a.coef = w.dd(D_KAPPA);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, false, clover ? (EPI_XPAY | EPI_CPOST) : EPI_XPAY, FIN_NONE, a));
+  }
+  // solution out
+  bool xdev = is_device_ptr(x);
+  void* xdst = x;
+  if (!xdev) {
+    QCU_CHECK(ctx->stage_out.ensure(full_c * 16 * nrhs, st));
+    xdst = ctx->stage_out.p;
+  }
+  QCU_CHECK_CUDA(launch_spinor_out(PREC_DOUBLE, g, nrhs, w.xhi.cview(0), xdst, full_c, st));
+  QCU_CHECK_CUDA(launch_spinor_out(PREC_DOUBLE, g, nrhs, w.xo.cview(0), static_cast<double2*>(xdst) + full_c / 2,
+                                   full_c, st));
+  ctx->launches += 3;
+  if (!xdev) QCU_CHECK_CUDA(cudaMemcpyAsync(x, xdst, full_c * 16 * nrhs, cudaMemcpyDeviceToHost, st));
+  QCU_CHECK_CUDA(cudaStreamSynchronize(st));
+  int ret = QCU_SUCCESS;
+  for (int r = 0; r < nrhs; r++) {
+    if (reports) {
+      reports[r].iterations = w.hi(I_ITERS)[r];
+      reports[r].reliable_updates = nupd[r];
+      reports[r].converged = conv[r];
+      reports[r].status = conv[r] ? QCU_SUCCESS : (status[r] != QCU_SUCCESS ? status[r] : QCU_ERR_NOT_CONVERGED);
+      reports[r].true_residual = true_res[r];
+      reports[r].kappa = kap[r];
+    }
+    if (!conv[r] && ret == QCU_SUCCESS) ret = status[r] != QCU_SUCCESS ? status[r] : QCU_ERR_NOT_CONVERGED;
+  }
+  if (ret != QCU_SUCCESS) set_error(ret, "not every right-hand side reached the tolerance");
+  return ret;
+}

@@ -1,0 +1,78 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the public
+headers declare (also the reference's C++ symbol names), and its host-side
+argument checks report errors instead of exiting. No compute call is made."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", "qcu.h"), os.path.join(ROOT, "include", "qcu_b200.h")]
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", src, flags=re.M):
+            name = m.group(1)
+            if name not in ("typedef", "struct"):
+                names.append(name)
+    return sorted(set(names))
+
+
+def exported(lib_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", lib_path], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_headers_declare_the_reference_interface():
+    names = declared_functions()
+    for ref_name in ("initGridSize", "dslashQcu", "fullDslashQcu", "cg_inverter", "loadQcuGauge", "invertCloverDslash"):
+        assert ref_name in names
+
+
+def test_library_exports_every_declared_symbol(qcu_lib):
+    syms = exported(qcu_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if n not in syms]
+    assert not missing, missing
+
+
+def test_library_exports_reference_cxx_names(qcu_lib):
+    syms = exported(qcu_lib.LIB_PATH)
+    for m in ("_Z18invertCloverDslashPvS_S_P10QcuParam_si", "_Z15preCloverDslashPvS_S_P10QcuParam_si",
+              "_Z20cloverDslashOneRoundPvS_S_P10QcuParam_si", "_Z24fullCloverDslashOneRoundPvS_S_P10QcuParam_si",
+              "_Z27newFullCloverDslashOneRoundPvS_S_P10QcuParam_si", "_Z13MmV_one_roundPvS_S_P10QcuParam_sS_"):
+        assert m in syms
+
+
+def test_library_loads_and_binds(qcu_lib):
+    L = qcu_lib.lib()
+    assert isinstance(L, ctypes.CDLL)
+
+
+def test_solve_param_defaults(qcu_lib):
+    sp = qcu_lib.solve_params()
+    assert sp.tol == 1e-10 and sp.bc_t == -1.0 and sp.precision == qcu_lib.PREC_HALF and sp.delta == 0.1
+
+
+def test_multi_rank_grid_is_rejected_without_exit(qcu_lib):
+    with pytest.raises(qcu_lib.QcuError) as e:
+        qcu_lib.initGridSize((2, 1, 1, 1), qcu_lib.param((8, 8, 8, 8)), None)
+    assert e.value.code == qcu_lib.QCU_ERR_UNSUPPORTED
+
+
+def test_calls_before_init_report_not_initialized(qcu_lib):
+    # no initGridSize in this process: every legacy entry returns early with a status
+    code = qcu_lib.lib().qcuPreCloverDslash(None, None, None, None, 0)
+    assert code == qcu_lib.QCU_ERR_NOT_INITIALIZED
+    assert qcu_lib.last_error()[0] == qcu_lib.QCU_ERR_NOT_INITIALIZED
+
+
+def test_bad_lattice_rejected(qcu_lib):
+    h = ctypes.c_void_p()
+    L4 = (ctypes.c_int * 4)(7, 8, 8, 8)  # odd Lx
+    assert qcu_lib.lib().qcuContextCreate(ctypes.byref(h), L4, 0) == qcu_lib.QCU_ERR_INVALID_ARG

@@ -1,0 +1,119 @@
+"""The even-odd mixed-precision CG (qcuInvert) on the GPU.
+
+Every solve is checked independently: the returned x is fed to the CPU
+oracle's full operator M = A - kappa D and |b - M x| / |b| must be below the
+requested tolerance (1e-10). Solutions are compared with the oracle's own FP64
+Schur solve at 1e-8 relative (both are solutions to 1e-10 of a system with a
+modest condition number).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to("cuda")
+
+
+def host(t, shape):
+    return t.cpu().numpy().reshape(shape)
+
+
+def true_residual(oracle, x, b, U, L, kappa, csw, bc=-1.0):
+    C = oracle.clover_build(U, L, kappa * csw)
+    r = b - oracle.apply_full(x, U, C, L, kappa, bc)
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("prec", ["double", "single", "half"])
+def test_config1_wilson_even_source(cuda, qcu_lib, oracle, prec):
+    """8^3x8 Wilson, kappa 0.12, no clover, antiperiodic t, eps 0.3, source on
+    the even sites only, stop at true residual 1e-10."""
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 1, 0.3)
+    b = oracle.full_spinor_random(L, 2)
+    b[1] = 0
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        x = dev(np.zeros_like(b))
+        rep = c.invert(x, dev(b), kappa=0.12, csw=0.0, bc_t=-1.0, tol=1e-10, precision=prec)[0]
+    xh = host(x, b.shape)
+    assert rep["converged"] and rep["true_residual"] < 1e-10
+    assert true_residual(oracle, xh, b, U, L, 0.12, 0.0) < 1e-10
+    xo, it, res = oracle.solve_schur(b, U, L, 0.12, 0.0, -1.0, 1e-11)
+    assert np.linalg.norm(xh - xo) / np.linalg.norm(xo) < 1e-8
+
+
+@pytest.mark.parametrize("prec", ["double", "single", "half"])
+def test_clover_solve(cuda, qcu_lib, oracle, prec):
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 3, 0.4)
+    b = oracle.full_spinor_random(L, 4)
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        x = dev(np.zeros_like(b))
+        rep = c.invert(x, dev(b), kappa=0.1375, csw=1.0, bc_t=-1.0, tol=1e-10, precision=prec)[0]
+    xh = host(x, b.shape)
+    assert rep["converged"], rep
+    assert true_residual(oracle, xh, b, U, L, 0.1375, 1.0) < 1e-10
+    if prec == "half":
+        assert rep["reliable_updates"] >= 2
+
+
+def test_multi_rhs_multi_kappa_equals_single(cuda, qcu_lib, oracle):
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 5, 0.4)
+    kappas = [0.1360, 0.1365, 0.1370, 0.1375]
+    bs = np.stack([oracle.full_spinor_random(L, 10 + r) for r in range(4)])
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        xb = dev(np.zeros_like(bs))
+        reps = c.invert(xb, dev(bs), nrhs=4, kappas=kappas, csw=1.0, tol=1e-10, precision="half")
+        xs = host(xb, bs.shape)
+        for r in range(4):
+            assert reps[r]["converged"]
+            assert true_residual(oracle, xs[r], bs[r], U, L, kappas[r], 1.0) < 1e-10
+            x1 = dev(np.zeros_like(bs[r]))
+            c.invert(x1, dev(bs[r]), kappa=kappas[r], csw=1.0, tol=1e-10, precision="half")
+            x1 = host(x1, bs[r].shape)
+            assert np.linalg.norm(xs[r] - x1) / np.linalg.norm(x1) < 1e-8
+
+
+def test_nan_source_is_rejected(cuda, qcu_lib, oracle):
+    L = (8, 8, 8, 8)
+    b = oracle.full_spinor_random(L, 4)
+    b[0, 3, 1, 2] = np.nan
+    with qcu_lib.Context(L) as c:
+        c.generate_gauge(1, 0.3)
+        with pytest.raises(qcu_lib.QcuError) as e:
+            c.invert(dev(np.zeros_like(b)), dev(b), kappa=0.12)
+        assert e.value.code == qcu_lib.QCU_ERR_INVALID_ARG
+
+
+def test_allocation_failure_is_reported(cuda, qcu_lib, oracle):
+    L = (8, 8, 8, 8)
+    b = oracle.full_spinor_random(L, 4)
+    q = qcu_lib
+    with q.Context(L) as c:
+        c.generate_gauge(1, 0.3)
+        q.lib().qcuDebugFailAllocAfter(3)
+        try:
+            with pytest.raises(q.QcuError) as e:
+                c.invert(dev(np.zeros_like(b)), dev(b), kappa=0.12, csw=1.0)
+            assert e.value.code == q.QCU_ERR_OUT_OF_MEMORY
+        finally:
+            q.lib().qcuDebugFailAllocAfter(-1)
+        # the context stays usable
+        x = dev(np.zeros_like(b))
+        rep = c.invert(x, dev(b), kappa=0.12, csw=1.0)[0]
+        assert rep["converged"]
+
+
+def test_kernel_launches_are_counted(cuda, qcu_lib):
+    with qcu_lib.Context((8, 8, 8, 8)) as c:
+        c.generate_gauge(1, 0.3)
+        n0 = c.launches
+        ms, nbytes = c.bench_stencil("half", 1, 1, 5)
+        assert c.launches > n0 and ms > 0 and nbytes > 0

@@ -1,0 +1,72 @@
+"""Pins the CPU oracle to the reference library itself (no GPU needed).
+
+The fixture tests/golden/ref_8x8x8x8.npz holds outputs of the unmodified
+reference library run on a B200 (tests/golden/make_golden.py): sampled entries
+plus whole-array checksums of every operator on seeded inputs. The oracle must
+reproduce them to FP64 rounding.
+"""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = os.path.join(HERE, "golden", "ref_8x8x8x8.npz")
+L = (8, 8, 8, 8)
+TOL = 1e-12  # relative, FP64
+
+
+@pytest.fixture(scope="module")
+def golden():
+    if not os.path.exists(FIX):
+        pytest.skip("golden fixture not generated yet (tests/golden/make_golden.py needs a GPU)")
+    return dict(np.load(FIX))
+
+
+@pytest.fixture(scope="module")
+def outputs(oracle):
+    U = oracle.gauge_random(L, 2024, 0.3)
+    psi = oracle.full_spinor_random(L, 11)
+    C = oracle.clover_build(U, L, 1.0)
+    Ci = oracle.clover_invert(C)
+    out = {}
+    for p in (0, 1):
+        out[f"dslash_p{p}"] = oracle.dslash(np.ascontiguousarray(psi[1 - p]), U, L, p)
+    for d in (0, 1):
+        out[f"full_d{d}"] = oracle.full_dslash_ref(psi, U, C, Ci, L, d)
+        out[f"newfull_d{d}"] = oracle.new_full_ref(psi, U, Ci, L, d)
+        rnd = np.stack([oracle.clover_apply(oracle.dslash(np.ascontiguousarray(psi[1 - p]), U, L, p, d),
+                                            np.ascontiguousarray(Ci[p])) for p in (0, 1)])
+        out[f"round_d{d}"] = rnd
+    out["invert"] = oracle.invert_clover_ref(psi, Ci, L)
+    out["pre"] = np.stack([oracle.clover_apply(np.ascontiguousarray(psi[p]), np.ascontiguousarray(C[p])) for p in (0, 1)])
+    out["mmv"] = oracle.mmv_ref(psi, U, Ci, L)
+    Up = oracle.gauge_pure(L, 7)
+    x, it, conv = oracle.cg_inverter_ref(psi, Up, L, 0)
+    out["cg_x"] = x
+    out["cg_meta"] = (it, conv)
+    return out
+
+
+NAMES = ["dslash_p0", "dslash_p1", "full_d0", "full_d1", "newfull_d0", "newfull_d1", "round_d0", "round_d1",
+         "invert", "pre", "mmv", "cg_x"]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_matches_reference(golden, outputs, name):
+    v = np.ascontiguousarray(outputs[name]).reshape(-1)
+    idx = golden[f"{name}__idx"]
+    ref = golden[f"{name}__val"]
+    scale = np.abs(ref).max()
+    assert np.abs(v[idx] - ref).max() <= TOL * scale * (1e3 if name == "cg_x" else 1.0)
+    n2 = float(golden[f"{name}__norm2"])
+    assert abs(np.vdot(v, v).real - n2) <= TOL * n2 * (1e3 if name == "cg_x" else 1.0)
+    w = np.cos(0.37 * np.arange(v.size))
+    ws = complex(golden[f"{name}__wsum"])
+    assert abs(np.sum(w * v) - ws) <= 1e-10 * np.sqrt(n2)
+
+
+def test_reference_cg_iteration_count(golden, outputs):
+    it, conv = outputs["cg_meta"]
+    assert bool(golden["cg_converged"]) and conv
+    assert abs(it - int(golden["cg_iterations"])) <= 1
