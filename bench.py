@@ -329,9 +329,27 @@ def run_reference(args, world, rank, local):
     return out
 
 
+def run_stencil(args):
+    """Times one fused stencil variant alone (Dslash GB/s of the metric), e.g.
+    for profiling: --stencil 24 24 24 48 --precision half --variant 2."""
+    import qcu_cg_inverter_b200 as q
+    hbm, src = peaks()
+    with q.Context(tuple(args.stencil), 0) as c:
+        c.generate_gauge(GAUGE_SEED, 0.5)
+        ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
+    gbs = nbytes / (ms / 1e3) / 1e9
+    print(json.dumps({"stencil": args.stencil, "precision": args.precision, "variant": args.variant,
+                      "nrhs": args.nrhs, "ms_per_launch": ms, "bytes_per_launch": nbytes, "GBps": gbs,
+                      "frac": gbs / hbm, "peak_source": src}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--stencil", type=int, nargs=4, default=None, help="time one stencil variant on this lattice")
+    ap.add_argument("--variant", type=int, default=2, help="0 hop, 1 hop+A^-1, 2 hop+A^-1+xpay+out2+norm")
+    ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -339,6 +357,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     args = ap.parse_args()
+    if args.stencil:
+        run_stencil(args)
+        return
     world, rank, local = dist_setup()
     if args.impl == "reference":
         out = run_reference(args, world, rank, local)

@@ -14,6 +14,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 FIX = os.path.join(HERE, "golden", "ref_8x8x8x8.npz")
 L = (8, 8, 8, 8)
 TOL = 1e-12  # relative, FP64
+# outputs that go through A^-1 at kappa*c_sw = 1, where clover blocks are
+# indefinite and ill-conditioned: the reference eliminates without pivoting,
+# the oracle with partial pivoting, so they agree to ~1e-11 there
+TOL_INV = 1e-10
+INVERSE_OUTPUTS = ("round_d0", "round_d1", "invert", "mmv", "newfull_d0", "newfull_d1")
 
 
 @pytest.fixture(scope="module")
@@ -57,10 +62,11 @@ def test_oracle_matches_reference(golden, outputs, name):
     v = np.ascontiguousarray(outputs[name]).reshape(-1)
     idx = golden[f"{name}__idx"]
     ref = golden[f"{name}__val"]
+    tol = {"cg_x": 1e-9}.get(name, TOL_INV if name in INVERSE_OUTPUTS else TOL)
     scale = np.abs(ref).max()
-    assert np.abs(v[idx] - ref).max() <= TOL * scale * (1e3 if name == "cg_x" else 1.0)
+    assert np.abs(v[idx] - ref).max() <= tol * scale
     n2 = float(golden[f"{name}__norm2"])
-    assert abs(np.vdot(v, v).real - n2) <= TOL * n2 * (1e3 if name == "cg_x" else 1.0)
+    assert abs(np.vdot(v, v).real - n2) <= tol * n2
     w = np.cos(0.37 * np.arange(v.size))
     ws = complex(golden[f"{name}__wsum"])
     assert abs(np.sum(w * v) - ws) <= 1e-10 * np.sqrt(n2)
