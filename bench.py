@@ -336,6 +336,8 @@ def run_stencil(args):
     hbm, src = peaks()
     with q.Context(tuple(args.stencil), 0) as c:
         c.generate_gauge(GAUGE_SEED, 0.5)
+        if args.sb:
+            c.set_shape(1, args.sb)
         ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
     gbs = nbytes / (ms / 1e3) / 1e9
     print(json.dumps({"stencil": args.stencil, "precision": args.precision, "variant": args.variant,
@@ -350,6 +352,7 @@ def main():
     ap.add_argument("--variant", type=int, default=2, help="0 hop, 1 hop+A^-1, 2 hop+A^-1+xpay+out2+norm")
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--sb", type=int, default=0, help="site lanes per block for --stencil (0 = library default)")
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

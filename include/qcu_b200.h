@@ -103,6 +103,9 @@ int qcuContextDestroy(qcu_context ctx);
 int qcuContextSetStream(qcu_context ctx, void* stream);
 /* The context's own stream (cudaStream_t), for recording events around calls. */
 void* qcuContextGetStream(qcu_context ctx);
+/* Thread-block shape (RHS lanes x site lanes, 32..256 threads) of the
+ * context's single-RHS kernels; the autotuner sets it from measurements. */
+int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes);
 /* Device bytes the context holds now. */
 long long qcuContextDeviceBytes(qcu_context ctx);
 

@@ -18,7 +18,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(HERE, "libqcu_b200.so")
+LIB_PATH = os.environ.get("QCU_B200_LIB", os.path.join(HERE, "libqcu_b200.so"))
 
 QCU_SUCCESS = 0
 QCU_ERR_INVALID_ARG = 1
@@ -105,6 +105,7 @@ def lib():
             "qcuContextDestroy": (i, [P]),
             "qcuContextSetStream": (i, [P, P]),
             "qcuContextGetStream": (P, [P]),
+            "qcuContextSetShape": (i, [P, i, i]),
             "qcuContextDeviceBytes": (ll, [P]),
             "qcuContextLaunchCount": (ll, [P]),
             "qcuLoadGauge": (i, [P, P]),
@@ -317,6 +318,10 @@ class Context:
         _check(lib().qcuBenchStencil(self._h, _PREC[precision], int(variant), int(nrhs), int(iters),
                                      ctypes.byref(ms), ctypes.byref(nbytes)))
         return ms.value, nbytes.value
+
+    def set_shape(self, rhs_lanes: int, site_lanes: int):
+        """Thread-block shape (RHS lanes x site lanes) of single-RHS kernels."""
+        _check(lib().qcuContextSetShape(self._h, int(rhs_lanes), int(site_lanes)))
 
     @property
     def stream(self) -> int:

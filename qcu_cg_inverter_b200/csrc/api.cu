@@ -483,6 +483,18 @@ int qcuContextSetStream(qcu_context ctx, void* stream) {
 
 void* qcuContextGetStream(qcu_context ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
+int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes) {
+  clear_error();
+  QCU_CHECK(ctx_check(ctx));
+  int n = rhs_lanes * site_lanes;
+  if (rhs_lanes < 1 || rhs_lanes > 32 || 32 % rhs_lanes || site_lanes < 1 || n % 32 || n > 256) {
+    set_error(QCU_ERR_INVALID_ARG, "block shape must have a power-of-two RHS width <= 32 and 32..256 threads");
+    return QCU_ERR_INVALID_ARG;
+  }
+  ctx->shape1 = LaunchShape{rhs_lanes, site_lanes};
+  return QCU_SUCCESS;
+}
+
 long long qcuContextDeviceBytes(qcu_context ctx) {
   if (!ctx) return 0;
   long long n = ctx->gauge64.bytes + ctx->gauge32.bytes + ctx->gauge16.bytes;

@@ -13,8 +13,17 @@ namespace qcu {
 
 typedef void (*DslashKernelFn)(const DslashArgs);
 
+// Minimum resident blocks (of up to 256 threads) per SM requested from the
+// register allocator: 2 caps the stencil at 128 registers. Measured on B200 at
+// 32^3x64 against no cap and an 85-register cap: equal or faster for every
+// precision and epilogue (16-bit fused: 203 vs 235 us; FP64 hop 232 vs 240
+// us), while 85 registers spill (FP64 hop 509 us).
+#ifndef QCU_DSLASH_MINB
+#define QCU_DSLASH_MINB 2
+#endif
+
 template <int P, bool DAG, int EPI, class Fin>
-__global__ void __launch_bounds__(256) dslash_kernel(const DslashArgs a) {
+__global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const DslashArgs a) {
   typedef typename CompReal<P>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;

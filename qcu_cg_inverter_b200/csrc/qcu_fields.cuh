@@ -60,10 +60,19 @@ template <> struct SpinorIO<PREC_SINGLE> {
   }
 };
 
-QCU_D float lo16(int w) { return (float)(short)(w & 0xffff); }
-QCU_D float hi16(int w) { return (float)(short)(w >> 16); }
-QCU_D int pack16(float a, float b) {
-  return (__float2int_rn(a) & 0xffff) | (__float2int_rn(b) << 16);
+// 16-bit fixed point <-> float without the conversion unit (I2F/F2I issue on
+// the quarter-rate XU pipe, which bounded the 16-bit stencil): a two's
+// complement v in [-32768, 32767], sign-flipped to v + 32768, is placed in the
+// mantissa of 2^23 (0x4B000000), so the float equals 2^23 + 32768 + v and one
+// exact subtraction recovers v. Encoding adds 1.5*2^23, which rounds to the
+// nearest integer (ties to even, as __float2int_rn) and leaves that integer's
+// two's complement in the low 16 bits of the float.
+QCU_D float lo16(int w) { return __uint_as_float(((unsigned)w & 0xffffu) ^ 0x4B008000u) - 8421376.0f; }
+QCU_D float hi16(int w) { return __uint_as_float(((unsigned)w >> 16) ^ 0x4B008000u) - 8421376.0f; }
+QCU_D int pack16(float a, float b) {  // |a|, |b| <= 32767.5
+  unsigned ia = __float_as_uint(a + 12582912.0f);
+  unsigned ib = __float_as_uint(b + 12582912.0f);
+  return (int)__byte_perm(ia, ib, 0x5410);
 }
 
 template <> struct SpinorIO<PREC_HALF> {

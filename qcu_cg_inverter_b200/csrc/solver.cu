@@ -29,8 +29,71 @@
 
 namespace qcu {
 
-enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_RES_R2, D_RES_AR2, D_RES_NE, D_BNORM, D_NUM };
-enum { I_ACTIVE = 0, I_EVENT, I_ITERS, I_BREAK, I_CIDX, I_UPD, I_ALL, I_NUM };
+enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_RES_R2, D_RES_AR2, D_RES_NE, D_BNORM,
+       D_TRUE, D_NUM };
+enum { I_ACTIVE = 0, I_EVENT, I_ITERS, I_BREAK, I_CIDX, I_UPD, I_RST, I_DONE, I_CONV, I_STATUS, I_NUPD, I_NUM };
+
+// Reliable-update control, entirely on the device (one thread per RHS), so an
+// update needs no host round trip:
+//   select: upd = !done && (paused itself || iteration cap reached)
+//   decide: after the FP64 residual kernels, per updated RHS either stop
+//           (converged / breakdown / cap) or restart the sloppy residual from
+//           r_ne with beta = |r_ne|^2/|r_old|^2 and a new trigger.
+struct RelParams {
+  double tol, delta2;
+  int maxiter;
+  int clover;
+};
+
+__global__ void rel_select_kernel(int nrhs, int* upd, const int* event, const int* done, const int* iters, int maxiter) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  upd[r] = (!done[r] && (event[r] || iters[r] >= maxiter)) ? 1 : 0;
+}
+
+__global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrhs) return;
+  double* D = dmem;
+  int* I = imem;
+#define DV(k) D[(size_t)(k) * nrhs + r]
+#define IV(k) I[(size_t)(k) * nrhs + r]
+  IV(I_RST) = 0;
+  if (!IV(I_UPD)) return;
+  IV(I_NUPD) += 1;
+  double ar2 = P.clover ? DV(D_RES_AR2) : DV(D_RES_R2);
+  double ne2 = DV(D_RES_NE);
+  double bn = DV(D_BNORM);
+  double res = bn > 0 ? sqrt(fmax(ar2, 0.0)) / bn : 0.0;
+  DV(D_TRUE) = res;
+  int stop = 0;
+  if (bn == 0.0 || res < P.tol) {
+    IV(I_CONV) = 1;
+    stop = 1;
+  } else if (!isfinite(res) || IV(I_BREAK)) {
+    IV(I_STATUS) = QCU_ERR_BREAKDOWN;
+    stop = 1;
+  } else if (IV(I_ITERS) >= P.maxiter) {
+    IV(I_STATUS) = QCU_ERR_NOT_CONVERGED;
+    stop = 1;
+  }
+  if (stop) {
+    IV(I_DONE) = 1;
+    IV(I_ACTIVE) = 0;
+    IV(I_EVENT) = 0;
+    return;
+  }
+  DV(D_BETA) = ne2 / DV(D_RROLD);  // rr_old = +inf before the first update -> beta = 0
+  DV(D_RR) = ne2;
+  double q = sqrt(fmax(ar2, 1e-300) / fmax(ne2, 1e-300));
+  double target = 0.5 * P.tol * bn / q;
+  DV(D_TRIG) = fmax(P.delta2 * ne2, target * target);
+  IV(I_ACTIVE) = 1;
+  IV(I_EVENT) = 0;
+  IV(I_RST) = 1;
+#undef DV
+#undef IV
+}
 
 struct SolverWorkspace {
   int nrhs = 0, ps = -1, pa = -1;
@@ -244,20 +307,19 @@ static int push_state(const OpCtx& o) {
   return QCU_SUCCESS;
 }
 
-static int run_chunk(const OpCtx& o, int K, bool graphs) {
+// Replays (capturing on first use) a CUDA graph of the work `enqueue` puts on
+// the stream; `key` identifies the sequence, `nlaunch` counts its kernels.
+template <class F>
+static int replay(const OpCtx& o, int key, bool graphs, long long nlaunch, F enqueue) {
   SolverWorkspace& w = *o.w;
-  if (!graphs) {
-    for (int k = 0; k < K; k++) QCU_CHECK(sloppy_iteration(o));
-    return QCU_SUCCESS;
-  }
+  if (!graphs) return enqueue();
   cudaGraphExec_t exec = nullptr;
   for (auto& g : w.graphs)
-    if (g.first == K) exec = g.second;
+    if (g.first == key) exec = g.second;
   if (!exec) {
     long long before = o.ctx->launches;
     QCU_CHECK_CUDA(cudaStreamBeginCapture(o.st, cudaStreamCaptureModeThreadLocal));
-    int s = QCU_SUCCESS;
-    for (int k = 0; k < K && s == QCU_SUCCESS; k++) s = sloppy_iteration(o);
+    int s = enqueue();
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(o.st, &graph);
     if (s != QCU_SUCCESS) {
@@ -268,11 +330,46 @@ static int run_chunk(const OpCtx& o, int K, bool graphs) {
     e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     QCU_CHECK_CUDA(e);
-    w.graphs.push_back({K, exec});
-    o.ctx->launches = before;  // captured launches are counted when replayed
+    w.graphs.push_back({key, exec});
+    o.ctx->launches = before;  // counted when replayed
   }
   QCU_CHECK_CUDA(cudaGraphLaunch(exec, o.st));
-  o.ctx->launches += 6LL * K;
+  o.ctx->launches += nlaunch;
+  return QCU_SUCCESS;
+}
+
+// K sloppy iterations as a sum of power-of-two graphs (no overshoot)
+static int run_chunk(const OpCtx& o, int K, bool graphs) {
+  for (int part = 32; part >= 1; part >>= 1) {
+    while (K >= part) {
+      QCU_CHECK(replay(o, part, graphs, 6LL * part, [&]() -> int {
+        for (int k = 0; k < part; k++) QCU_CHECK(sloppy_iteration(o));
+        return QCU_SUCCESS;
+      }));
+      K -= part;
+    }
+  }
+  return QCU_SUCCESS;
+}
+
+// select + FP64 residual + decide + restart, all on the device
+static int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select) {
+  SolverWorkspace& w = *o.w;
+  const int nrhs = w.nrhs;
+  const int tb = 32, nb = (nrhs + tb - 1) / tb;
+  if (select) {
+    rel_select_kernel<<<nb, tb, 0, o.st>>>(nrhs, w.di(I_UPD), w.di(I_EVENT), w.di(I_DONE), w.di(I_ITERS), P.maxiter);
+    QCU_CHECK_CUDA(cudaGetLastError());
+    o.ctx->launches++;
+  }
+  QCU_CHECK(reliable_update(o));
+  rel_decide_kernel<<<nb, tb, 0, o.st>>>(nrhs, w.mem.as<double>(), w.di(0), P);
+  QCU_CHECK_CUDA(cudaGetLastError());
+  const int Vh = o.ctx->g.Vh;
+  QCU_CHECK_CUDA(launch_convert(w.pa, PREC_DOUBLE, Vh, nrhs, w.rlo.view(0), w.z64.cview(0), w.di(I_RST), nullptr,
+                                w.shape, o.st));
+  QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, Vh, nrhs, w.p.view(0), w.rlo.cview(0), w.dd(D_BETA), w.di(I_RST), w.shape, o.st));
+  o.ctx->launches += 3;
   return QCU_SUCCESS;
 }
 
@@ -340,9 +437,9 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
   for (int r = 0; r < nrhs; r++) {
     w.hd(D_KAPPA)[r] = kap[r];
     w.hd(D_MK2)[r] = -kap[r] * kap[r];
+    w.hd(D_RROLD)[r] = INFINITY;
     w.hi(I_CIDX)[r] = cidx[r];
     w.hi(I_UPD)[r] = 1;
-    w.hi(I_ALL)[r] = 1;
   }
   QCU_CHECK(push_state(o));
 
@@ -367,18 +464,17 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
                                    cudaMemcpyDeviceToHost, st));
     QCU_CHECK_CUDA(cudaStreamSynchronize(st));
   }
-  std::vector<double> bnorm(nrhs);
   for (int r = 0; r < nrhs; r++) {
     double b2 = ctx->red.host.as<double>()[2 * r];
     if (!isfinite(b2)) {
       set_error(QCU_ERR_INVALID_ARG, "source contains NaN or Inf");
       return QCU_ERR_INVALID_ARG;
     }
-    bnorm[r] = sqrt(b2);
+    w.hd(D_BNORM)[r] = sqrt(b2);
   }
+  QCU_CHECK(push_state(o));
   // bhat = A_ee^-1 (b_e + kappa D_eo A_oo^-1 b_o)
   {
-    Field* bo = &w.b2;
     DslashArgs a;
     if (clover) {
       QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, g, 1, nrhs, w.b2.cview(1), w.t64.view(0),
@@ -388,108 +484,76 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
       a = op_args(o, PREC_DOUBLE, 0, w.t64, w.bh, nullptr);
     } else {
       a = op_args(o, PREC_DOUBLE, 0, w.b2, w.bh, nullptr);
-      a.in = bo->cview(1);
+      a.in = w.b2.cview(1);
     }
     a.x = w.b2.cview(0);
     a.coef = w.dd(D_KAPPA);
     QCU_CHECK(dsl(o, PREC_DOUBLE, false, clover ? (EPI_XPAY | EPI_CPOST) : EPI_XPAY, FIN_NONE, a));
   }
-  // x = 0 everywhere; the first "reliable update" computes r_ne = Mhat^dag bhat
+  // x = 0; the first update (all RHS) computes r_ne = Mhat^dag bhat and p = r
   QCU_CHECK_CUDA(cudaMemsetAsync(w.xhi.data.p, 0, w.xhi.data.bytes, st));
   QCU_CHECK_CUDA(cudaMemsetAsync(w.xlo.data.p, 0, w.xlo.data.bytes, st));
   QCU_CHECK_CUDA(cudaMemsetAsync(w.p.data.p, 0, w.p.data.bytes, st));
   if (w.p.norm.p) QCU_CHECK_CUDA(cudaMemsetAsync(w.p.norm.p, 0, w.p.norm.bytes, st));
 
   const double delta = P.delta > 0 && P.delta < 1 ? P.delta : (P.precision == QCU_PREC_DOUBLE ? 1e-2 : 0.1);
-  std::vector<int> done(nrhs, 0), conv(nrhs, 0), nupd(nrhs, 0), status(nrhs, QCU_SUCCESS);
-  std::vector<double> true_res(nrhs, 1.0), rr_at_check(nrhs, 0.0);
-  std::vector<int> it_at_check(nrhs, 0);
-  bool first = true;
-  int K = 8;
+  RelParams RP{P.tol, delta * delta, P.maxiter, clover ? 1 : 0};
   const bool graphs = P.use_graphs != 0;
-  for (int guard = 0; guard < 1000000; guard++) {
-    // ---- reliable updates / convergence checks for the RHS in I_UPD ----
-    bool any_upd = false;
-    for (int r = 0; r < nrhs; r++) any_upd |= w.hi(I_UPD)[r] != 0;
-    if (any_upd) {
-      QCU_CHECK(push_state(o));
-      QCU_CHECK(reliable_update(o));
-      QCU_CHECK(pull_state(o));
-      bool any_restart = false;
-      for (int r = 0; r < nrhs; r++) {
-        if (!w.hi(I_UPD)[r]) continue;
-        nupd[r]++;
-        double ar2 = clover ? w.hd(D_RES_AR2)[r] : w.hd(D_RES_R2)[r];
-        double ne2 = w.hd(D_RES_NE)[r];
-        double res = bnorm[r] > 0 ? sqrt(fmax(ar2, 0.0)) / bnorm[r] : 0.0;
-        true_res[r] = res;
-        bool stop = false;
-        if (bnorm[r] == 0.0 || res < P.tol) {
-          conv[r] = 1;
-          stop = true;
-        } else if (!isfinite(res) || w.hi(I_BREAK)[r]) {
-          status[r] = QCU_ERR_BREAKDOWN;
-          stop = true;
-        } else if (w.hi(I_ITERS)[r] >= P.maxiter) {
-          status[r] = QCU_ERR_NOT_CONVERGED;
-          stop = true;
-        }
-        if (stop) {
-          done[r] = 1;
-          w.hi(I_ACTIVE)[r] = 0;
-          w.hi(I_EVENT)[r] = 0;
-          w.hi(I_UPD)[r] = 0;
-          continue;
-        }
-        // continue: r_lo = r_ne, beta = |r_ne|^2 / rr_old, rr = |r_ne|^2
-        w.hd(D_BETA)[r] = first ? 0.0 : ne2 / w.hd(D_RROLD)[r];
-        w.hd(D_RR)[r] = ne2;
-        // next check when the iterated residual fell by delta, or earlier
-        // when the predicted true residual reaches tol
-        double q = sqrt(fmax(ar2, 1e-300) / fmax(ne2, 1e-300));
-        double target = 0.5 * P.tol * bnorm[r] / q;
-        w.hd(D_TRIG)[r] = fmax(delta * delta * ne2, target * target);
-        w.hi(I_ACTIVE)[r] = 1;
-        w.hi(I_EVENT)[r] = 0;
-        rr_at_check[r] = ne2;
-        it_at_check[r] = w.hi(I_ITERS)[r];
-        any_restart = true;
-      }
-      if (any_restart) {
-        QCU_CHECK(push_state(o));
-        // r_lo = r_ne and p = r_lo + beta p for the restarted RHS (mask I_UPD)
-        QCU_CHECK_CUDA(launch_convert(w.pa, PREC_DOUBLE, g.Vh, nrhs, w.rlo.view(0), w.z64.cview(0), w.di(I_UPD), nullptr,
-                                      w.shape, st));
-        QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, g.Vh, nrhs, w.p.view(0), w.rlo.cview(0), w.dd(D_BETA), w.di(I_UPD),
-                                   w.shape, st));
-        ctx->launches += 2;
-      }
-      for (int r = 0; r < nrhs; r++) w.hi(I_UPD)[r] = 0;
-      QCU_CHECK(push_state(o));
-      first = false;
-    }
-    bool any_active = false;
-    for (int r = 0; r < nrhs; r++) any_active |= (!done[r] && w.hi(I_ACTIVE)[r]);
-    if (!any_active) break;
-    // ---- a chunk of sloppy iterations ----
-    QCU_CHECK(run_chunk(o, K, graphs));
-    QCU_CHECK(pull_state(o));
-    // next chunk length from the observed convergence rate
-    double need = 64;
+  QCU_CHECK(enqueue_reliable(o, RP, false));
+  QCU_CHECK(pull_state(o));
+  // chunk lengths from each RHS's observed convergence rate
+  std::vector<double> rate(nrhs, 0.0), last_rr(nrhs, -1.0);
+  std::vector<int> last_it(nrhs, -1);
+  for (int loop = 0; loop < 10000000; loop++) {
+    int n_left = 0, n_iter = 0;
     for (int r = 0; r < nrhs; r++) {
-      if (done[r]) continue;
-      if (w.hi(I_EVENT)[r] || w.hi(I_ITERS)[r] >= P.maxiter) w.hi(I_UPD)[r] = 1;
-      if (!w.hi(I_ACTIVE)[r]) continue;
-      int di = w.hi(I_ITERS)[r] - it_at_check[r];
-      double rr = w.hd(D_RR)[r], tr = w.hd(D_TRIG)[r];
-      if (di > 0 && rr < rr_at_check[r] && rr > tr) {
-        double rate = log(rr / rr_at_check[r]) / di;
-        need = fmin(need, log(tr / rr) / rate);
+      if (w.hi(I_DONE)[r]) continue;
+      n_left++;
+      if (w.hi(I_ACTIVE)[r]) n_iter++;
+    }
+    if (n_left == 0) break;
+    if (n_iter > 0) {
+      double need = 1e30;
+      bool known = false;
+      for (int r = 0; r < nrhs; r++) {
+        if (w.hi(I_DONE)[r] || !w.hi(I_ACTIVE)[r]) continue;
+        double rr = w.hd(D_RR)[r], tr = w.hd(D_TRIG)[r];
+        if (rate[r] < 0 && rr > tr) {
+          need = fmin(need, log(tr / rr) / rate[r]);
+          known = true;
+        }
+        need = fmin(need, (double)(P.maxiter - w.hi(I_ITERS)[r]));
+      }
+      int K = known ? (int)ceil(need) : 4;
+      K = std::max(1, std::min(K, 64));
+      QCU_CHECK(run_chunk(o, K, graphs));
+      QCU_CHECK(pull_state(o));
+      for (int r = 0; r < nrhs; r++) {
+        int it = w.hi(I_ITERS)[r];
+        double rr = w.hd(D_RR)[r];
+        if (last_it[r] >= 0 && it > last_it[r] && rr > 0 && last_rr[r] > 0 && rr < last_rr[r])
+          rate[r] = log(rr / last_rr[r]) / (it - last_it[r]);
+        last_it[r] = it;
+        last_rr[r] = rr;
       }
     }
-    int k2 = 4;
-    while (k2 < 64 && k2 < need) k2 *= 2;
-    K = k2;
+    bool any_upd = false, all_upd = true;
+    for (int r = 0; r < nrhs; r++) {
+      if (w.hi(I_DONE)[r]) continue;
+      bool u = w.hi(I_EVENT)[r] || w.hi(I_ITERS)[r] >= P.maxiter;
+      any_upd |= u;
+      all_upd &= u;
+    }
+    if (!any_upd && n_iter == 0) {  // cannot happen: a paused RHS always carries its event
+      set_error(QCU_ERR_BREAKDOWN, "solver state stalled");
+      return QCU_ERR_BREAKDOWN;
+    }
+    if (any_upd) {
+      QCU_CHECK(replay(o, -1, graphs, 0, [&]() -> int { return enqueue_reliable(o, RP, true); }));
+      for (int r = 0; r < nrhs; r++)
+        if (!w.hi(I_DONE)[r] && (w.hi(I_EVENT)[r] || w.hi(I_ITERS)[r] >= P.maxiter)) last_it[r] = -1;  // rr restarts
+      if (all_upd) QCU_CHECK(pull_state(o));  // nothing iterates until the update is known
+    }
   }
   // x_e += x_lo (no-op for checked RHS), x_o = A_oo^-1 (b_o + kappa D_oe x_e)
   for (int r = 0; r < nrhs; r++) w.hi(I_UPD)[r] = 1;
@@ -514,17 +578,20 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
   ctx->launches += 3;
   if (!xdev) QCU_CHECK_CUDA(cudaMemcpyAsync(x, xdst, full_c * 16 * nrhs, cudaMemcpyDeviceToHost, st));
   QCU_CHECK_CUDA(cudaStreamSynchronize(st));
+  QCU_CHECK(pull_state(o));
   int ret = QCU_SUCCESS;
   for (int r = 0; r < nrhs; r++) {
+    int conv = w.hi(I_CONV)[r];
+    int stat = w.hi(I_STATUS)[r];
     if (reports) {
       reports[r].iterations = w.hi(I_ITERS)[r];
-      reports[r].reliable_updates = nupd[r];
-      reports[r].converged = conv[r];
-      reports[r].status = conv[r] ? QCU_SUCCESS : (status[r] != QCU_SUCCESS ? status[r] : QCU_ERR_NOT_CONVERGED);
-      reports[r].true_residual = true_res[r];
+      reports[r].reliable_updates = w.hi(I_NUPD)[r];
+      reports[r].converged = conv;
+      reports[r].status = conv ? QCU_SUCCESS : (stat != QCU_SUCCESS ? stat : QCU_ERR_NOT_CONVERGED);
+      reports[r].true_residual = w.hd(D_TRUE)[r];
       reports[r].kappa = kap[r];
     }
-    if (!conv[r] && ret == QCU_SUCCESS) ret = status[r] != QCU_SUCCESS ? status[r] : QCU_ERR_NOT_CONVERGED;
+    if (!conv && ret == QCU_SUCCESS) ret = stat != QCU_SUCCESS ? stat : QCU_ERR_NOT_CONVERGED;
   }
   if (ret != QCU_SUCCESS) set_error(ret, "not every right-hand side reached the tolerance");
   return ret;
