@@ -122,6 +122,17 @@ int qcuGenerateSpinor(qcu_context ctx, void* out, int nrhs, unsigned long long s
 /* out (half spinor, parity) = D^(dag) in (half spinor, 1-parity), hopping
  * term with time boundary factor bc_t. */
 int qcuDslash(qcu_context ctx, void* out, const void* in, int parity, int dagger, double bc_t);
+/* Same result as qcuDslash, for callers that must not allocate device memory
+ * during the call (a framework that already holds the GPU's memory in its own
+ * pool, or a loop that cannot take cudaMalloc's implicit synchronisation).
+ * No counterpart in the reference. Instead of the staging fields qcuDslash
+ * allocates on first use, it uses a fixed 6 MiB scratch array compiled into
+ * the library (held on every GPU that loads it), so the lattice's half volume
+ * may be at most 16384 sites (larger: QCU_ERR_INVALID_ARG). in/out must be
+ * device pointers. Calls that overlap on the GPU share that array and race.
+ * The first call on a device looks up the array's device address; make that
+ * first call before starting any stream capture. */
+int qcuDslashNoAlloc(qcu_context ctx, void* out, const void* in, int parity, int dagger, double bc_t);
 /* out = A in (inverse = 0) or A^-1 in (inverse = 1), full spinors, with
  * A = 1 + csw_eff*T (csw_eff = kappa*c_sw; 1 reproduces the reference). */
 int qcuApplyClover(qcu_context ctx, void* out, const void* in, double csw_eff, int inverse);

@@ -113,6 +113,7 @@ def lib():
             "qcuExportGauge": (i, [P, P]),
             "qcuGenerateSpinor": (i, [P, P, i, ctypes.c_ulonglong]),
             "qcuDslash": (i, [P, P, P, i, i, d]),
+            "qcuDslashNoAlloc": (i, [P, P, P, i, i, d]),
             "qcuApplyClover": (i, [P, P, P, d, i]),
             "qcuApplyOperator": (i, [P, P, P, d, d, d, i]),
             "qcuInvert": (i, [P, P, P, i, ctypes.POINTER(d), ctypes.POINTER(SolveParams),
