@@ -55,12 +55,20 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons around the timed region.
+
+    Started before the warm-up and given time to produce its first sample;
+    samples every 20 ms with timestamps; mark() brackets the timed region and
+    summary() keeps the samples inside it (or, if the region was shorter than
+    one period, the nearest samples on either side)."""
+
+    REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -68,13 +76,23 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "--query-gpu=timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            deadline = time.time() + 5
+            while time.time() < deadline and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
+
+    def start(self):
+        self.t0 = time.time()
+
+    def stop(self):
+        self.t1 = time.time()
+        time.sleep(0.05)
 
     def __exit__(self, *a):
         if self.proc:
@@ -85,25 +103,31 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
+        import datetime
+        rows = []
         try:
             for line in open(self.path):
                 f = [v.strip() for v in line.split(",")]
-                if len(f) < 7:
+                if len(f) < 8:
                     continue
                 try:
-                    sm.append(float(f[0]))
-                    mx.append(float(f[1]))
+                    ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    rows.append((ts, float(f[1]), float(f[2]), f[4:8]))
                 except ValueError:
                     continue
-                for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[3:7]):
-                    if v.lower().startswith("active"):
-                        reasons.add(name)
             os.unlink(self.path)
         except Exception:
             pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if self.t0 is not None and self.t0 <= r[0] <= (self.t1 or r[0])]
+        sel = inside
+        if not sel and rows and self.t0 is not None:
+            before = [r for r in rows if r[0] < self.t0]
+            after = [r for r in rows if r[0] > (self.t1 or self.t0)]
+            sel = before[-1:] + after[:1]
+        reasons = sorted({n for r in sel for n, v in zip(self.REASONS, r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median([r[1] for r in sel]) if sel else None,
+                "sm_max_mhz": max(r[2] for r in sel) if sel else None, "reasons": reasons,
+                "samples_in_timed_region": len(inside), "samples_used": len(sel)}
 
 
 def dist_setup():
@@ -196,14 +220,16 @@ def run_ours(args, world, rank, local):
             total += e0.elapsed_time(e1) / 1e3
         return total, rep
 
-    # warm-up (also builds the clover fields and captures the CUDA graphs)
-    for _ in range(args.warmup):
-        solve(x, b, args.precision)
-    barrier(world, device)
-    torch.cuda.synchronize(device)
-    n0 = ctx.launches
     with ClockSampler(local) as clk:
+        # warm-up (also autotunes, builds the clover fields and captures the CUDA graphs)
+        for _ in range(args.warmup):
+            solve(x, b, args.precision)
+        barrier(world, device)
+        torch.cuda.synchronize(device)
+        n0 = ctx.launches
+        clk.start()
         t_mixed, rep = timed(lambda: solve(x, b, args.precision), args.steps)
+        clk.stop()
     launches = (ctx.launches - n0) // max(args.steps, 1)
     t_mixed = max_over_ranks(t_mixed, world, device)
     barrier(world, device)
@@ -329,6 +355,86 @@ def run_reference(args, world, rank, local):
     return out
 
 
+MULTI_LATTICE = (24, 24, 24, 48)
+MULTI_KAPPAS = (0.1360, 0.1365, 0.1370, 0.1375)
+MULTI_EPS = 0.4  # not fixed by the workload description; recorded in the output
+
+
+def point_sources(torch, V, site, device):
+    """12 spin-colour point sources at checkerboard site `site` of parity 0,
+    as full spinors [rhs][parity][Vh][4][3] (complex128)."""
+    Vh = V // 2
+    b = torch.zeros(12, 2, Vh, 12, dtype=torch.complex128, device=device)
+    for k in range(12):
+        b[k, 0, site, k] = 1.0
+    return b.reshape(12, -1)
+
+
+def run_multi(args):
+    """The multi-RHS batch: 24^3x48 Wilson-clover (c_sw 1), 12 point sources at
+    a seeded site x 4 kappas = 48 RHS, one mixed-precision batched solve (each
+    RHS stops on its own at true residual 1e-10) against the plain FP64
+    single-RHS CG on the same GPU (a sample of RHS solved one at a time, one
+    per kappa, scaled to 48)."""
+    import random
+
+    import torch
+
+    import qcu_cg_inverter_b200 as q
+    device = torch.device("cuda", 0)
+    ctx = q.Context(MULTI_LATTICE, 0)
+    ctx.generate_gauge(GAUGE_SEED, MULTI_EPS)
+    V = ctx.volume
+    site = random.Random(SOURCE_SEED).randrange(V // 2)
+    src12 = point_sources(torch, V, site, device)
+    nr = 12 * len(MULTI_KAPPAS)
+    b = src12.repeat(len(MULTI_KAPPAS), 1).contiguous()
+    kap = [k for k in MULTI_KAPPAS for _ in range(12)]
+    x = torch.zeros_like(b)
+    kw = dict(csw=CSW, bc_t=BC_T, tol=TOL)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+
+    def timed(fn):
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, r
+
+    # warm-up: autotune and clover for every kappa, graphs
+    ctx.invert(x, b, nrhs=nr, kappas=kap, precision=args.precision, **kw)
+    n0 = ctx.launches
+    t_multi, reps = timed(lambda: ctx.invert(x, b, nrhs=nr, kappas=kap, precision=args.precision, **kw))
+    launches = ctx.launches - n0
+    assert all(r["converged"] for r in reps), reps
+    # FP64 single-RHS sample: spin-colour 0 for each kappa
+    x1 = torch.zeros_like(b[0])
+    ctx.invert(x1, b[0].contiguous(), kappa=MULTI_KAPPAS[0], precision="double", **kw)
+    t64, it64 = [], []
+    for j, k in enumerate(MULTI_KAPPAS):
+        bb = b[12 * j].contiguous()
+        t, r = timed(lambda: ctx.invert(x1, bb, kappa=k, precision="double", **kw)[0])
+        assert r["converged"], r
+        t64.append(t)
+        it64.append(r["iterations"])
+    per64 = sum(t64) / len(t64)
+    ctx.close()
+    out = {
+        "workload": "24^3x48 Wilson-clover multi-RHS: 12 point sources x 4 kappas = 48 RHS, true residual 1e-10",
+        "lattice": MULTI_LATTICE, "kappas": MULTI_KAPPAS, "csw": CSW, "eps": MULTI_EPS, "source_site": site,
+        "precision": args.precision, "nrhs": nr,
+        "multi_s": t_multi, "multi_per_rhs_s": t_multi / nr,
+        "iterations": [r["iterations"] for r in reps], "max_true_residual": max(r["true_residual"] for r in reps),
+        "fp64_single_rhs_s": per64, "fp64_single_iterations": it64,
+        "fp64_single_total_48_s": per64 * nr,
+        "speedup_vs_fp64_single": per64 * nr / t_multi,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(out), flush=True)
+
+
 def run_stencil(args):
     """Times one fused stencil variant alone (Dslash GB/s of the metric), e.g.
     for profiling: --stencil 24 24 24 48 --precision half --variant 2."""
@@ -353,7 +459,8 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--sb", type=int, default=0, help="site lanes per block for --stencil (0 = library default)")
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--multi", action="store_true", help="the 48-RHS 24^3x48 batch against FP64 single-RHS")
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="half", choices=["half", "single", "double"])
@@ -362,6 +469,9 @@ def main():
     args = ap.parse_args()
     if args.stencil:
         run_stencil(args)
+        return
+    if args.multi:
+        run_multi(args)
         return
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -81,6 +81,8 @@ typedef struct {
   double delta;       /* reliable-update factor: the true residual is recomputed in
                          FP64 when the iterated one fell by this factor (0 = default) */
   int use_graphs;     /* replay CUDA graphs of the inner iterations (1 = yes) */
+  int autotune;       /* time the launch shapes for this (precision, nrhs) before the
+                         first solve that uses them (1 = yes; see qcuAutotune) */
 } qcu_solve_params;
 
 typedef struct {
@@ -154,6 +156,12 @@ int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, const double* k
  * context stream; *bytes receives the algorithmic bytes of one launch. */
 int qcuBenchStencil(qcu_context ctx, int precision, int variant, int nrhs, int iters, double* ms_per_launch,
                     double* bytes);
+
+/* Autotuner: times the fused stencil over every launch shape (RHS lanes x
+ * site lanes) for this precision and number of right-hand sides on the
+ * context's lattice, keeps the fastest for the solver, and reports it. With
+ * QCU_TUNE_CACHE=<file> the choice is appended to that file and reused. */
+int qcuAutotune(qcu_context ctx, int precision, int nrhs, int* rhs_lanes, int* site_lanes, double* ms);
 
 /* Number of kernels this library enqueued since the context was created. */
 long long qcuContextLaunchCount(qcu_context ctx);

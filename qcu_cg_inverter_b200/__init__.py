@@ -55,7 +55,7 @@ class QcuGrid(ctypes.Structure):
 class SolveParams(ctypes.Structure):
     _fields_ = [("kappa", ctypes.c_double), ("csw", ctypes.c_double), ("bc_t", ctypes.c_double),
                 ("tol", ctypes.c_double), ("maxiter", ctypes.c_int), ("precision", ctypes.c_int),
-                ("delta", ctypes.c_double), ("use_graphs", ctypes.c_int)]
+                ("delta", ctypes.c_double), ("use_graphs", ctypes.c_int), ("autotune", ctypes.c_int)]
 
 
 class SolveReport(ctypes.Structure):
@@ -120,6 +120,7 @@ def lib():
                               ctypes.POINTER(SolveReport)]),
             "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
             "qcuDebugFailAllocAfter": (None, [ll]),
+            "qcuAutotune": (i, [P, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(d)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -323,6 +324,13 @@ class Context:
     def set_shape(self, rhs_lanes: int, site_lanes: int):
         """Thread-block shape (RHS lanes x site lanes) of single-RHS kernels."""
         _check(lib().qcuContextSetShape(self._h, int(rhs_lanes), int(site_lanes)))
+
+    def autotune(self, precision, nrhs: int = 1):
+        """Times every launch shape for (precision, nrhs); returns (Rb, Sb, ms)."""
+        rb, sb, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+        _check(lib().qcuAutotune(self._h, _PREC[precision], int(nrhs), ctypes.byref(rb), ctypes.byref(sb),
+                                 ctypes.byref(ms)))
+        return rb.value, sb.value, ms.value
 
     @property
     def stream(self) -> int:

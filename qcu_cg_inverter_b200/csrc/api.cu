@@ -201,6 +201,7 @@ int ctx_clover_reserve(qcu_context ctx, int nslots) {
   B.stamp.resize(nslots, 0);
   B.pinned.resize(nslots, 0);
   B.capacity = nslots;
+  ctx->clover_gen++;  // device addresses changed: captured graphs are stale
   return QCU_SUCCESS;
 }
 
@@ -424,6 +425,7 @@ void qcuSolveParamsDefault(qcu_solve_params* p) {
   p->precision = QCU_PREC_HALF;
   p->delta = 0.1;
   p->use_graphs = 1;
+  p->autotune = 1;
 }
 
 int qcuContextCreate(qcu_context* out, const int lattice[4], int device) {

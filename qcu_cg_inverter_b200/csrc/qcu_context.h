@@ -130,6 +130,9 @@ struct qcu_context_s {
   qcu::DevBuf stage_in, stage_out;  // device staging of host arguments
   qcu::DevBuf status;               // clover build status counters
   qcu::SolverWorkspace* solver = nullptr;  // owned; freed by qcuContextDestroy (solver.cu)
+  std::map<std::pair<int, int>, qcu::LaunchShape> tuned;  // (precision, nrhs) -> block shape (tune.cu)
+  bool tune_cache_loaded = false;
+  long long clover_gen = 0;  // bumped whenever the clover bank moves
   long long launches = 0;
   ~qcu_context_s();
 };
@@ -143,6 +146,11 @@ int ctx_clover_reserve(qcu_context ctx, int nslots);
 const void* ctx_clover_ptr(qcu_context ctx, int prec, bool inverse);
 size_t ctx_clover_stride(qcu_context ctx, int prec);
 const void* ctx_gauge(qcu_context ctx, int prec);
+
+// launch shapes (tune.cu)
+LaunchShape ctx_shape(qcu_context ctx, int prec, int nrhs);
+bool ctx_is_tuned(qcu_context ctx, int prec, int nrhs);
+int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms);
 
 // staging of user pointers that may live on the host
 bool is_device_ptr(const void* p);

@@ -107,6 +107,7 @@ struct SolverWorkspace {
   CgDevState st;
   LaunchShape shape{1, 128};
   std::vector<std::pair<int, cudaGraphExec_t>> graphs;
+  long long graph_gen = -1;  // clover bank generation the graphs were captured against
   ~SolverWorkspace() { drop_graphs(); }
   void drop_graphs() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
@@ -119,20 +120,16 @@ struct SolverWorkspace {
   size_t mem_bytes() const { return (size_t)D_NUM * nrhs * sizeof(double) + (size_t)I_NUM * nrhs * sizeof(int); }
 };
 
-static LaunchShape shape_for(int nrhs) {
-  if (nrhs <= 1) return LaunchShape{1, 128};
-  int rb = 1;
-  while (rb * 2 <= nrhs && rb * 2 <= 8) rb *= 2;
-  return LaunchShape{rb, 128 / rb};
-}
-
 static int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover) {
   cudaStream_t st = ctx->stream;
   const int pa = (ps == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
   const int vp = ctx->g.Vh_pad;
-  if (w.nrhs != nrhs || w.ps != ps || w.vh_pad != vp) w.drop_graphs();
+  if (w.nrhs != nrhs || w.ps != ps || w.vh_pad != vp || w.graph_gen != ctx->clover_gen) w.drop_graphs();
+  w.graph_gen = ctx->clover_gen;
   w.clover = clover;
-  w.shape = shape_for(nrhs);
+  LaunchShape sh = ctx_shape(ctx, ps, nrhs);
+  if (sh.Rb != w.shape.Rb || sh.Sb != w.shape.Sb) w.drop_graphs();
+  w.shape = sh;
   QCU_CHECK(w.b2.alloc(PREC_DOUBLE, vp, nrhs, 2, st));
   for (Field* f : {&w.bh, &w.xhi, &w.t64, &w.y64, &w.u64, &w.z64, &w.xo}) QCU_CHECK(f->alloc(PREC_DOUBLE, vp, nrhs, 1, st));
   QCU_CHECK(w.xlo.alloc(pa, vp, nrhs, 1, st));
@@ -427,6 +424,7 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
       cidx[r] = slot;
     }
   }
+  if (P.autotune && !ctx_is_tuned(ctx, P.precision, nrhs)) QCU_CHECK(ctx_autotune(ctx, P.precision, nrhs, nullptr));
   if (!ctx->solver) ctx->solver = new SolverWorkspace();
   SolverWorkspace& w = *ctx->solver;
   QCU_CHECK(ws_prepare(ctx, w, nrhs, P.precision, clover));
