@@ -255,6 +255,8 @@ def run_ours(args, world, rank, local):
         hbm, src = peaks()
         roof = q.Context(ROOF_LATTICE, local)
         roof.generate_gauge(GAUGE_SEED, 0.5)
+        for p in ("half", "double"):
+            roof.autotune(p, 1)
         ms, nbytes = roof.bench_stencil("half", 2, 1, 50)
         ms_hop64, bytes_hop64 = roof.bench_stencil("double", 0, 1, 20)
         ms_hop16, bytes_hop16 = roof.bench_stencil("half", 0, 1, 50)
@@ -444,6 +446,8 @@ def run_stencil(args):
         c.generate_gauge(GAUGE_SEED, 0.5)
         if args.sb:
             c.set_shape(1, args.sb)
+        else:
+            c.autotune(args.precision, args.nrhs)
         ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
     gbs = nbytes / (ms / 1e3) / 1e9
     print(json.dumps({"stencil": args.stencil, "precision": args.precision, "variant": args.variant,

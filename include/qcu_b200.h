@@ -95,7 +95,8 @@ typedef struct {
 } qcu_solve_report;
 
 /* Fills params with the defaults: kappa 0.12, csw 0, bc_t -1, tol 1e-10,
- * maxiter 20000, precision half, delta 0.1, use_graphs 1. */
+ * maxiter 20000, precision half, delta 0 (= 1e-2 for 16-bit inner storage,
+ * 1e-3 for single and double), use_graphs 1, autotune 1. */
 void qcuSolveParamsDefault(qcu_solve_params* params);
 
 int qcuContextCreate(qcu_context* ctx, const int lattice[4], int device);
@@ -108,6 +109,10 @@ void* qcuContextGetStream(qcu_context ctx);
 /* Thread-block shape (RHS lanes x site lanes, 32..256 threads) of the
  * context's single-RHS kernels; the autotuner sets it from measurements. */
 int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes);
+/* Storage behind QCU_PREC_HALF: fast_links = 1 (default) keeps 16-bit spinors
+ * with FP32 links (all 18 reals, nothing to decode or rebuild) and an FP32
+ * clover inverse; 0 keeps links and clover in 16-bit too (smallest footprint). */
+int qcuContextSetHalfOperator(qcu_context ctx, int fast_links);
 /* Device bytes the context holds now. */
 long long qcuContextDeviceBytes(qcu_context ctx);
 

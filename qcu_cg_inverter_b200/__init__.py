@@ -106,6 +106,7 @@ def lib():
             "qcuContextSetStream": (i, [P, P]),
             "qcuContextGetStream": (P, [P]),
             "qcuContextSetShape": (i, [P, i, i]),
+            "qcuContextSetHalfOperator": (i, [P, i]),
             "qcuContextDeviceBytes": (ll, [P]),
             "qcuContextLaunchCount": (ll, [P]),
             "qcuLoadGauge": (i, [P, P]),
@@ -324,6 +325,10 @@ class Context:
     def set_shape(self, rhs_lanes: int, site_lanes: int):
         """Thread-block shape (RHS lanes x site lanes) of single-RHS kernels."""
         _check(lib().qcuContextSetShape(self._h, int(rhs_lanes), int(site_lanes)))
+
+    def set_half_operator(self, fast_links: bool):
+        """16-bit solver storage: FP32 links/clover (True, default) or 16-bit (False)."""
+        _check(lib().qcuContextSetHalfOperator(self._h, int(bool(fast_links))))
 
     def autotune(self, precision, nrhs: int = 1):
         """Times every launch shape for (precision, nrhs); returns (Rb, Sb, ms)."""

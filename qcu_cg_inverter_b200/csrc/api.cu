@@ -146,8 +146,13 @@ int ctx_check(qcu_context ctx) {
   return QCU_SUCCESS;
 }
 
-const void* ctx_gauge(qcu_context ctx, int prec) {
-  return prec == PREC_DOUBLE ? ctx->gauge64.p : (prec == PREC_SINGLE ? ctx->gauge32.p : ctx->gauge16.p);
+const void* ctx_gauge(qcu_context ctx, int op) {
+  switch (op_link_format(op)) {
+    case PREC_DOUBLE: return ctx->gauge64.p;
+    case PREC_SINGLE: return ctx->gauge32.p;
+    case PREC_HALF: return ctx->gauge16.p;
+    default: return ctx->gauge18.p;
+  }
 }
 
 static int ingest_gauge(qcu_context ctx, const void* gauge) {
@@ -155,6 +160,7 @@ static int ingest_gauge(qcu_context ctx, const void* gauge) {
   QCU_CHECK(ctx->gauge64.ensure(gauge_field_bytes(PREC_DOUBLE, g.Vh_pad), ctx->stream));
   QCU_CHECK(ctx->gauge32.ensure(gauge_field_bytes(PREC_SINGLE, g.Vh_pad), ctx->stream));
   QCU_CHECK(ctx->gauge16.ensure(gauge_field_bytes(PREC_HALF, g.Vh_pad), ctx->stream));
+  QCU_CHECK(ctx->gauge18.ensure(gauge_field_bytes(LINK_SINGLE18, g.Vh_pad), ctx->stream));
   const void* src = gauge;
   size_t aos_bytes = (size_t)8 * g.Vh * 9 * 16;
   if (!is_device_ptr(gauge)) {
@@ -162,7 +168,8 @@ static int ingest_gauge(qcu_context ctx, const void* gauge) {
     QCU_CHECK_CUDA(cudaMemcpyAsync(ctx->stage_in.p, gauge, aos_bytes, cudaMemcpyHostToDevice, ctx->stream));
     src = ctx->stage_in.p;
   }
-  QCU_CHECK_CUDA(launch_gauge_ingest(g, src, ctx->gauge64.p, ctx->gauge32.p, ctx->gauge16.p, ctx->stream));
+  QCU_CHECK_CUDA(launch_gauge_ingest(g, src, ctx->gauge64.p, ctx->gauge32.p, ctx->gauge16.p, ctx->gauge18.p,
+                                     ctx->stream));
   ctx->launches++;
   ctx->gauge_loaded = true;
   ctx->gauge_version++;
@@ -249,14 +256,16 @@ int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot) {
   return QCU_SUCCESS;
 }
 
-const void* ctx_clover_ptr(qcu_context ctx, int prec, bool inverse) {
+const void* ctx_clover_ptr(qcu_context ctx, int op, bool inverse) {
   CloverBank& B = ctx->clover;
   if (!inverse) return B.A64.p;
-  return prec == PREC_DOUBLE ? B.Ainv64.p : (prec == PREC_SINGLE ? B.Ainv32.p : B.Ainv16.p);
+  const int pc = op_clover_prec(op);
+  return pc == PREC_DOUBLE ? B.Ainv64.p : (pc == PREC_SINGLE ? B.Ainv32.p : B.Ainv16.p);
 }
-size_t ctx_clover_stride(qcu_context ctx, int prec) {
+size_t ctx_clover_stride(qcu_context ctx, int op) {
   CloverBank& B = ctx->clover;
-  return prec == PREC_DOUBLE ? B.b64 : (prec == PREC_SINGLE ? B.b32 : B.b16);
+  const int pc = op_clover_prec(op);
+  return pc == PREC_DOUBLE ? B.b64 : (pc == PREC_SINGLE ? B.b32 : B.b16);
 }
 
 // slot-offset clover pointer
@@ -423,7 +432,7 @@ void qcuSolveParamsDefault(qcu_solve_params* p) {
   p->tol = 1e-10;
   p->maxiter = 20000;
   p->precision = QCU_PREC_HALF;
-  p->delta = 0.1;
+  p->delta = 0.0;  // per-precision default (1e-2 for 16-bit, 1e-3 otherwise)
   p->use_graphs = 1;
   p->autotune = 1;
 }
@@ -494,6 +503,14 @@ int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes) {
     return QCU_ERR_INVALID_ARG;
   }
   ctx->shape1 = LaunchShape{rhs_lanes, site_lanes};
+  ctx->shape_set = true;
+  return QCU_SUCCESS;
+}
+
+int qcuContextSetHalfOperator(qcu_context ctx, int fast_links) {
+  clear_error();
+  QCU_CHECK(ctx_check(ctx));
+  ctx->half_op = fast_links ? OP_HALF_FAST : OP_HALF;
   return QCU_SUCCESS;
 }
 

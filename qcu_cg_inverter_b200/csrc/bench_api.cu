@@ -43,7 +43,9 @@ extern "C" int qcuExportGauge(qcu_context ctx, void* out) {
 }
 
 static int spinor_b(int prec) { return prec == PREC_DOUBLE ? 192 : (prec == PREC_SINGLE ? 96 : 52); }
-static int link_b(int prec) { return prec == PREC_DOUBLE ? 96 : (prec == PREC_SINGLE ? 48 : 24); }
+static int link_b(int fmt) {
+  return fmt == PREC_DOUBLE ? 96 : (fmt == PREC_SINGLE ? 48 : (fmt == PREC_HALF ? 24 : 72));  // 18 FP32 reals
+}
 static int clov_b(int prec) { return prec == PREC_DOUBLE ? 576 : (prec == PREC_SINGLE ? 288 : 148); }
 
 extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs, int iters, double* ms_per_launch,
@@ -60,6 +62,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   }
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
+  const int op = ctx_op(ctx, prec);  // the operator variant the solver uses for this precision
   Field fin, fout, fx, fout2;
   QCU_CHECK(fin.alloc(prec, g.Vh_pad, nrhs, 1, st));
   QCU_CHECK(fout.alloc(prec, g.Vh_pad, nrhs, 1, st));
@@ -77,12 +80,9 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   int slot = 0;
   if (variant >= 1) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
   QCU_CHECK(ctx->red.ensure(g, nrhs, st));
-  LaunchShape sh = ctx->shape1;
-  if (nrhs > 1) {
-    int rb = 1;
-    while (rb * 2 <= nrhs && rb * 2 <= 8) rb *= 2;
-    sh = LaunchShape{rb, 128 / rb};
-  }
+  // the shape the solver would use (tuned when qcuAutotune ran, else the
+  // default), unless qcuContextSetShape overrode the single-RHS shape
+  LaunchShape sh = (nrhs == 1 && ctx->shape_set) ? ctx->shape1 : ctx_shape(ctx, op, nrhs);
   DslashArgs a;
   memset(&a, 0, sizeof(a));
   a.g = g;
@@ -92,18 +92,18 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   a.out = fout.view(0);
   a.x = fx.cview(0);
   a.out2 = fout2.view(0);
-  a.gauge = ctx_gauge(ctx, prec);
-  a.clover = static_cast<const char*>(ctx_clover_ptr(ctx, prec, true)) + ctx_clover_stride(ctx, prec) * slot;
+  a.gauge = ctx_gauge(ctx, op);
+  a.clover = static_cast<const char*>(ctx_clover_ptr(ctx, op, true)) + ctx_clover_stride(ctx, op) * slot;
   a.coef0 = -0.0169;
   a.bc_t = -1.0;
   a.red = ctx->red.args();
   int epi = variant == 0 ? 0 : (variant == 1 ? EPI_CPRE : (EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM));
-  for (int k = 0; k < 3; k++) QCU_CHECK_CUDA(launch_dslash(prec, false, epi, FIN_NONE, a, sh, st));
+  for (int k = 0; k < 3; k++) QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
   cudaEvent_t e0, e1;
   QCU_CHECK_CUDA(cudaEventCreate(&e0));
   QCU_CHECK_CUDA(cudaEventCreate(&e1));
   QCU_CHECK_CUDA(cudaEventRecord(e0, st));
-  for (int k = 0; k < iters; k++) QCU_CHECK_CUDA(launch_dslash(prec, false, epi, FIN_NONE, a, sh, st));
+  for (int k = 0; k < iters; k++) QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
   QCU_CHECK_CUDA(cudaEventRecord(e1, st));
   QCU_CHECK_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -115,7 +115,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   if (bytes) {
     double per_rhs = 8.0 * spinor_b(prec) + spinor_b(prec);
     if (variant == 2) per_rhs += 2.0 * spinor_b(prec);  // xpay input + second output
-    double shared = 8.0 * link_b(prec) + (variant >= 1 ? clov_b(prec) : 0.0);
+    double shared = 8.0 * link_b(op_link_format(op)) + (variant >= 1 ? clov_b(op_clover_prec(op)) : 0.0);
     int tiles = (nrhs + sh.Rb - 1) / sh.Rb;
     *bytes = (double)g.Vh * (nrhs * per_rhs + tiles * shared);
   }

@@ -15,7 +15,8 @@ namespace qcu {
 // ---------------------------------------------------------------------------
 // gauge: AoS FP64 -> internal (up to three precisions in one pass)
 // ---------------------------------------------------------------------------
-__global__ void gauge_aos_to_internal_kernel(Geom g, const double2* __restrict__ src, void* d64, void* d32, void* d16) {
+__global__ void gauge_aos_to_internal_kernel(Geom g, const double2* __restrict__ src, void* d64, void* d32, void* d16,
+                                             void* d18) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;  // link index over [dir][parity][Vh]
   if (l >= 8 * g.Vh) return;
   const int mp = l / g.Vh, s = l - mp * g.Vh;
@@ -30,11 +31,17 @@ __global__ void gauge_aos_to_internal_kernel(Geom g, const double2* __restrict__
   if (d64) LinkIO<PREC_DOUBLE>::store(d64, g.Vh_pad, mu, parity, s, U);
   if (d32) LinkIO<PREC_SINGLE>::store(d32, g.Vh_pad, mu, parity, s, U);
   if (d16) LinkIO<PREC_HALF>::store(d16, g.Vh_pad, mu, parity, s, U);
+  if (d18) {  // third row rebuilt in FP64 as everywhere else, then stored
+    su3_reconstruct(U);
+    LinkIO<LINK_SINGLE18>::store(d18, g.Vh_pad, mu, parity, s, U);
+  }
 }
 
-cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, cudaStream_t st) {
+cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, void* d18,
+                                cudaStream_t st) {
   int n = 8 * g.Vh;
-  gauge_aos_to_internal_kernel<<<(n + 127) / 128, 128, 0, st>>>(g, static_cast<const double2*>(aos), d64, d32, d16);
+  gauge_aos_to_internal_kernel<<<(n + 127) / 128, 128, 0, st>>>(g, static_cast<const double2*>(aos), d64, d32, d16,
+                                                                  d18);
   return cudaGetLastError();
 }
 

@@ -137,6 +137,23 @@ QCU_HD size_t chunk_index(int c, int s, int r, int NC, int nrhs) {
 // ---------------------------------------------------------------------------
 enum Prec : int { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
 
+// Link storage formats (LinkIO): the three above keep 12 reals (two rows) and
+// rebuild the third row; LINK_SINGLE18 keeps all 18 reals in FP32 (80 bytes
+// with padding), so a kernel does no decoding and no reconstruction.
+enum LinkFormat : int { LINK_SINGLE18 = 3 };
+
+// Operator variants (the `prec` argument of launch_dslash): spinor, link and
+// clover storage of one stencil instantiation.
+enum OpVariant : int {
+  OP_DOUBLE = 0,     // FP64 spinors, FP64 12-real links, FP64 clover
+  OP_SINGLE = 1,     // FP32 spinors, FP32 12-real links, FP32 clover
+  OP_HALF = 2,       // 16-bit spinors, 16-bit 12-real links, 16-bit clover
+  OP_HALF_FAST = 3,  // 16-bit spinors, FP32 18-real links, FP32 clover
+};
+__host__ __device__ constexpr int op_spinor_prec(int op) { return op == OP_HALF_FAST ? (int)PREC_HALF : op; }
+__host__ __device__ constexpr int op_link_format(int op) { return op == OP_HALF_FAST ? (int)LINK_SINGLE18 : op; }
+__host__ __device__ constexpr int op_clover_prec(int op) { return op == OP_HALF_FAST ? (int)PREC_SINGLE : op; }
+
 // 16-bit storage is fixed point: a real v in [-1,1] is stored as
 // round(v*32767); spinors and clover blocks carry one float norm per site so
 // that their largest component maps to 1.

@@ -116,8 +116,10 @@ struct qcu_context_s {
   cudaStream_t stream = nullptr;
   int L[4] = {0, 0, 0, 0};
   qcu::Geom g{};
-  // resident gauge field (internal layout) in three precisions
-  qcu::DevBuf gauge64, gauge32, gauge16;
+  // resident gauge field (internal layout): 12-real double/single/16-bit and
+  // 18-real single (the fast 16-bit operator's links)
+  qcu::DevBuf gauge64, gauge32, gauge16, gauge18;
+  int half_op = qcu::OP_HALF_FAST;  // operator variant behind QCU_PREC_HALF
   bool gauge_loaded = false;
   long long gauge_version = 0;
   const void* legacy_gauge_src = nullptr;  // AoS pointer last ingested by the legacy API
@@ -125,6 +127,7 @@ struct qcu_context_s {
   long long clock = 0;
   qcu::Scratch red;
   qcu::LaunchShape shape1{1, 128};  // single-RHS stencil/BLAS shape
+  bool shape_set = false;           // shape1 set by qcuContextSetShape
   // scratch fields for the legacy and operator entry points
   qcu::Field lin, lout, ltmp, ltmp2, lx;
   qcu::DevBuf stage_in, stage_out;  // device staging of host arguments
@@ -139,13 +142,16 @@ struct qcu_context_s {
 
 namespace qcu {
 
-// context helpers (api.cu)
+// context helpers (api.cu). `op` arguments are OpVariant values (PREC_*
+// values are the matching uniform variants).
 int ctx_check(qcu_context ctx);
 int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot);  // builds on demand
 int ctx_clover_reserve(qcu_context ctx, int nslots);
-const void* ctx_clover_ptr(qcu_context ctx, int prec, bool inverse);
-size_t ctx_clover_stride(qcu_context ctx, int prec);
-const void* ctx_gauge(qcu_context ctx, int prec);
+const void* ctx_clover_ptr(qcu_context ctx, int op, bool inverse);
+size_t ctx_clover_stride(qcu_context ctx, int op);
+const void* ctx_gauge(qcu_context ctx, int op);
+// the operator variant that serves spinor precision `prec`
+inline int ctx_op(qcu_context ctx, int prec) { return prec == PREC_HALF ? ctx->half_op : prec; }
 
 // launch shapes (tune.cu)
 LaunchShape ctx_shape(qcu_context ctx, int prec, int nrhs);
@@ -156,7 +162,8 @@ int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms);
 bool is_device_ptr(const void* p);
 
 // kernel launchers (defined in the .cu files)
-cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, cudaStream_t st);
+cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, void* d18,
+                                cudaStream_t st);
 cudaError_t launch_spinor_in(int prec, const Geom& g, int nrhs, const void* aos, size_t aos_stride, SpinorView dst,
                              cudaStream_t st);
 cudaError_t launch_spinor_out(int prec, const Geom& g, int nrhs, CSpinorView src, void* aos, size_t aos_stride,

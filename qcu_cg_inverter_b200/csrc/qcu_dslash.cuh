@@ -93,43 +93,63 @@ template <class R> QCU_D void scale_half(Half2<R>& h, R s) {
   for (int c = 0; c < 3; c++) { h.h0[c] = s * h.h0[c]; h.h1[c] = s * h.h1[c]; }
 }
 
-// One direction (both hops) of the stencil.
-template <int P, int MU, int F, class R>
+// Loads the neighbour spinor and projects it, times `phase` (the time
+// boundary factor, or 1). For 16-bit storage the per-site norm is applied to
+// the six projected components instead of the twelve stored ones.
+template <int PS, int MU, bool FWD, int F, class R>
+QCU_D void load_project(Half2<R>& h, const CSpinorView& in, int s, int r, R phase) {
+  if constexpr (PS == PREC_HALF) {
+    Spinor<float> raw;
+    float nm = SpinorIO<PREC_HALF>::load_raw(raw, in, s, r) * (float)phase;
+    Half2<float> hf;
+    project<MU, FWD, F>(hf, raw);
+    scale_half(hf, nm);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      h.h0[c] = mk((R)hf.h0[c].re, (R)hf.h0[c].im);
+      h.h1[c] = mk((R)hf.h1[c].re, (R)hf.h1[c].im);
+    }
+  } else {
+    Spinor<R> p;
+    SpinorIO<PS>::load(p, in, s, r);
+    project<MU, FWD, F>(h, p);
+    if (MU == 3 && phase != R(1)) scale_half(h, phase);
+  }
+}
+
+// One direction (both hops) of the stencil: PS = spinor precision, PL = link
+// storage format.
+template <int PS, int PL, int MU, int F, class R>
 QCU_D void hop_dir(Spinor<R>& o, const Geom& g, const Nbrs& nb, int parity, int s, int r,
                    const CSpinorView& in, const void* gauge, R bc_t) {
   Link<R> U;
-  Spinor<R> p;
   Half2<R> h;
   Cplx<R> a[3], b[3];
   // forward: U_mu(x) in(x+mu)
-  LinkIO<P>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  SpinorIO<P>::load(p, in, nb.fwd[MU], r);
-  project<MU, true, F>(h, p);
-  if (MU == 3 && nb.t == g.Lt - 1) scale_half(h, bc_t);
+  LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
+  load_project<PS, MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : R(1));
   su3_mul(a, U, h.h0);
   su3_mul(b, U, h.h1);
   reconstruct<MU, true, F>(o, a, b);
   // backward: U_mu(x-mu)^dag in(x-mu); the link lives on the other parity
-  LinkIO<P>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  SpinorIO<P>::load(p, in, nb.bwd[MU], r);
-  project<MU, false, F>(h, p);
-  if (MU == 3 && nb.t == 0) scale_half(h, bc_t);
+  LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
+  load_project<PS, MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : R(1));
   su3_dag_mul(a, U, h.h0);
   su3_dag_mul(b, U, h.h1);
   reconstruct<MU, false, F>(o, a, b);
 }
 
-template <int P, bool DAG, class R>
+template <int PS, int PL, bool DAG, class R>
 QCU_D void hop(Spinor<R>& o, const Geom& g, int parity, int s, int r, const CSpinorView& in,
                const void* gauge, R bc_t) {
   constexpr int F = DAG ? -1 : 1;
 #pragma unroll
   for (int k = 0; k < 12; k++) o.c[k] = mk(R(0), R(0));
   const Nbrs nb = neighbours(g, s, parity);
-  hop_dir<P, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<P, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<P, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<P, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
 }
 
 }  // namespace qcu

@@ -22,38 +22,40 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #define QCU_DSLASH_MINB 2
 #endif
 
-template <int P, bool DAG, int EPI, class Fin>
+// OP selects the storage of spinors, links and clover (OpVariant).
+template <int OP, bool DAG, int EPI, class Fin>
 __global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const DslashArgs a) {
-  typedef typename CompReal<P>::type R;
+  constexpr int PS = op_spinor_prec(OP), PL = op_link_format(OP), PC = op_clover_prec(OP);
+  typedef typename CompReal<PS>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
   const bool valid = (s < a.g.Vh) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
   double nrm = 0.0;
   if (valid) {
     Spinor<R> o;
-    hop<P, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
+    hop<PS, PL, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
     const void* clov = a.clover;
     if (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) {
       if (a.clover_idx) clov = static_cast<const char*>(a.clover) + a.clover_stride * (size_t)a.clover_idx[r];
     }
-    if (EPI & EPI_CPRE) clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
+    if (EPI & EPI_CPRE) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     if (EPI & EPI_XPAY) {
       const R c = a.coef ? (R)a.coef[r] : (R)a.coef0;
       Spinor<R> xv;
-      SpinorIO<P>::load(xv, a.x, s, r);
-      if (EPI & EPI_CX) clover_apply_site<P>(xv, clov, a.g.Vh_pad, a.parity, s);
+      SpinorIO<PS>::load(xv, a.x, s, r);
+      if (EPI & EPI_CX) clover_apply_site<PC>(xv, clov, a.g.Vh_pad, a.parity, s);
 #pragma unroll
       for (int k = 0; k < 12; k++) o.c[k] = xv.c[k] + c * o.c[k];
-      if (EPI & EPI_CPOST) clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
+      if (EPI & EPI_CPOST) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     }
-    SpinorIO<P>::store(a.out, s, r, o);
+    SpinorIO<PS>::store(a.out, s, r, o);
     if (EPI & EPI_NORM) {
 #pragma unroll
       for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
     }
     if (EPI & EPI_OUT2) {
-      clover_apply_site<P>(o, clov, a.g.Vh_pad, a.parity, s);
-      SpinorIO<P>::store(a.out2, s, r, o);
+      clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
+      SpinorIO<PS>::store(a.out2, s, r, o);
     }
   }
   if (EPI & EPI_NORM) {

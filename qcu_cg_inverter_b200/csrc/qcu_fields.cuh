@@ -77,6 +77,19 @@ QCU_D int pack16(float a, float b) {  // |a|, |b| <= 32767.5
 
 template <> struct SpinorIO<PREC_HALF> {
   typedef float R;
+  // integer-valued components (not yet scaled) and the factor that scales them
+  static QCU_D float load_raw(Spinor<R>& v, const CSpinorView& f, int s, int r) {
+    const int4* p = static_cast<const int4*>(f.data);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int4 w = p[chunk_index(c, s, r, 3, f.nrhs)];
+      v.c[4 * c + 0] = mk(lo16(w.x), hi16(w.x));
+      v.c[4 * c + 1] = mk(lo16(w.y), hi16(w.y));
+      v.c[4 * c + 2] = mk(lo16(w.z), hi16(w.z));
+      v.c[4 * c + 3] = mk(lo16(w.w), hi16(w.w));
+    }
+    return f.norm[(size_t)s * f.nrhs + r] * kInvFix;
+  }
   static QCU_D void load(Spinor<R>& v, const CSpinorView& f, int s, int r) {
     const int4* p = static_cast<const int4*>(f.data);
     float nm = f.norm[(size_t)s * f.nrhs + r] * kInvFix;
@@ -174,6 +187,34 @@ template <> struct LinkIO<PREC_HALF> {
       w.y = pack16((float)L.u[2 * c + 1].re * kFix, (float)L.u[2 * c + 1].im * kFix);
       p[chunk_index(c, s, 0, 3, 1)] = w;
     }
+  }
+};
+
+// All 18 reals in FP32: 5 chunks of float4 (the last half used). Nothing to
+// decode or rebuild; 80 bytes per link, shared by every RHS lane of a site.
+template <> struct LinkIO<LINK_SINGLE18> {
+  typedef float R;
+  static QCU_D void load(Link<R>& L, const void* gauge, int Vh_pad, int mu, int parity, int s) {
+    const float4* p = static_cast<const float4*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 5;
+    float4 w[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) w[c] = __ldg(p + chunk_index(c, s, 0, 5, 1));
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      L.u[2 * c] = mk(w[c].x, w[c].y);
+      L.u[2 * c + 1] = mk(w[c].z, w[c].w);
+    }
+    L.u[8] = mk(w[4].x, w[4].y);
+  }
+  // L must hold all nine entries (third row rebuilt)
+  template <class RS>
+  static QCU_D void store(void* gauge, int Vh_pad, int mu, int parity, int s, const Link<RS>& L) {
+    float4* p = static_cast<float4*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 5;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+      p[chunk_index(c, s, 0, 5, 1)] = make_float4((float)L.u[2 * c].re, (float)L.u[2 * c].im,
+                                                  (float)L.u[2 * c + 1].re, (float)L.u[2 * c + 1].im);
+    p[chunk_index(4, s, 0, 5, 1)] = make_float4((float)L.u[8].re, (float)L.u[8].im, 0.f, 0.f);
   }
 };
 
@@ -365,6 +406,7 @@ inline size_t clover_field_bytes(int P, int Vh_pad) {
   return (size_t)2 * Vh_pad * 9 * 16 + (size_t)2 * Vh_pad * 4;
 }
 inline size_t gauge_field_bytes(int P, int Vh_pad) {
+  if (P == LINK_SINGLE18) return (size_t)8 * Vh_pad * 5 * 16;
   if (P == PREC_DOUBLE) return (size_t)8 * Vh_pad * 6 * 16;
   if (P == PREC_SINGLE) return (size_t)8 * Vh_pad * 3 * 16;
   return (size_t)8 * Vh_pad * 3 * 8;

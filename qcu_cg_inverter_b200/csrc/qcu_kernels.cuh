@@ -51,7 +51,9 @@ struct LaunchShape {
   int Rb, Sb;
 };
 
-cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape shape,
+// `op` is an OpVariant (spinor / link / clover storage); the pointers in `a`
+// must be fields of those formats.
+cudaError_t launch_dslash(int op, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape shape,
                           cudaStream_t stream);
 
 // Number of blocks along x for a field of Vh sites.

@@ -50,9 +50,13 @@ bool ctx_is_tuned(qcu_context ctx, int prec, int nrhs) {
   return ctx->tuned.count(std::make_pair(prec, nrhs)) != 0;
 }
 
-int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms) {
+// `spinor_prec` is the public precision; the timed operator is the variant
+// that serves it (ctx_op), and the result is kept under that variant.
+int ctx_autotune(qcu_context ctx, int spinor_prec, int nrhs, double* best_ms) {
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
+  const int op = ctx_op(ctx, spinor_prec);
+  const int prec = op_spinor_prec(op);
   if (!ctx->gauge_loaded) {
     set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
     return QCU_ERR_NOT_INITIALIZED;
@@ -82,8 +86,8 @@ int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms) {
   a.out = fout.view(0);
   a.x = fx.cview(0);
   a.out2 = fout2.view(0);
-  a.gauge = ctx_gauge(ctx, prec);
-  a.clover = static_cast<const char*>(ctx_clover_ptr(ctx, prec, true)) + ctx_clover_stride(ctx, prec) * slot;
+  a.gauge = ctx_gauge(ctx, op);
+  a.clover = static_cast<const char*>(ctx_clover_ptr(ctx, op, true)) + ctx_clover_stride(ctx, op) * slot;
   a.coef0 = -0.0169;
   a.bc_t = -1.0;
   a.red = ctx->red.args();
@@ -97,14 +101,14 @@ int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms) {
     for (int threads : {64, 128, 256}) {
       if (threads % rb) continue;
       LaunchShape sh{rb, threads / rb};
-      if (launch_dslash(prec, false, epi, FIN_NONE, a, sh, st) != cudaSuccess) {
+      if (launch_dslash(op, false, epi, FIN_NONE, a, sh, st) != cudaSuccess) {
         (void)cudaGetLastError();
         continue;
       }
-      QCU_CHECK_CUDA(launch_dslash(prec, false, epi, FIN_NONE, a, sh, st));
+      QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
       QCU_CHECK_CUDA(cudaEventRecord(e0, st));
       const int reps = 5;
-      for (int k = 0; k < reps; k++) QCU_CHECK_CUDA(launch_dslash(prec, false, epi, FIN_NONE, a, sh, st));
+      for (int k = 0; k < reps; k++) QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
       QCU_CHECK_CUDA(cudaEventRecord(e1, st));
       QCU_CHECK_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
@@ -118,13 +122,13 @@ int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  ctx->tuned[std::make_pair(prec, nrhs)] = best;
+  ctx->tuned[std::make_pair(op, nrhs)] = best;
   if (best_ms) *best_ms = best_t;
   const char* path = getenv("QCU_TUNE_CACHE");
   if (path) {
     FILE* f = fopen(path, "a");
     if (f) {
-      fprintf(f, "%d %d %d %d %d %d %d %d %.6f\n", ctx->L[0], ctx->L[1], ctx->L[2], ctx->L[3], prec, nrhs, best.Rb,
+      fprintf(f, "%d %d %d %d %d %d %d %d %.6f\n", ctx->L[0], ctx->L[1], ctx->L[2], ctx->L[3], op, nrhs, best.Rb,
               best.Sb, best_t);
       fclose(f);
     }
@@ -144,7 +148,7 @@ extern "C" int qcuAutotune(qcu_context ctx, int precision, int nrhs, int* rhs_la
     return QCU_ERR_INVALID_ARG;
   }
   QCU_CHECK(ctx_autotune(ctx, precision, nrhs, ms));
-  LaunchShape sh = ctx_shape(ctx, precision, nrhs);
+  LaunchShape sh = ctx_shape(ctx, ctx_op(ctx, precision), nrhs);
   if (rhs_lanes) *rhs_lanes = sh.Rb;
   if (site_lanes) *site_lanes = sh.Sb;
   return QCU_SUCCESS;

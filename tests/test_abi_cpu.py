@@ -56,7 +56,8 @@ def test_library_loads_and_binds(qcu_lib):
 
 def test_solve_param_defaults(qcu_lib):
     sp = qcu_lib.solve_params()
-    assert sp.tol == 1e-10 and sp.bc_t == -1.0 and sp.precision == qcu_lib.PREC_HALF and sp.delta == 0.1
+    assert sp.tol == 1e-10 and sp.bc_t == -1.0 and sp.precision == qcu_lib.PREC_HALF and sp.delta == 0.0
+    assert sp.use_graphs == 1 and sp.autotune == 1
 
 
 def test_multi_rank_grid_is_rejected_without_exit(qcu_lib):

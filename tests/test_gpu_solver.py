@@ -46,13 +46,17 @@ def test_config1_wilson_even_source(cuda, qcu_lib, oracle, prec):
     assert np.linalg.norm(xh - xo) / np.linalg.norm(xo) < 1e-8
 
 
-@pytest.mark.parametrize("prec", ["double", "single", "half"])
+@pytest.mark.parametrize("prec", ["double", "single", "half", "half-compact"])
 def test_clover_solve(cuda, qcu_lib, oracle, prec):
+    """half = 16-bit spinors with FP32 links/clover; half-compact = all 16-bit."""
     L = (8, 8, 8, 8)
     U = oracle.gauge_random(L, 3, 0.4)
     b = oracle.full_spinor_random(L, 4)
     with qcu_lib.Context(L) as c:
         c.load_gauge(dev(U))
+        if prec == "half-compact":
+            c.set_half_operator(False)
+            prec = "half"
         x = dev(np.zeros_like(b))
         rep = c.invert(x, dev(b), kappa=0.1375, csw=1.0, bc_t=-1.0, tol=1e-10, precision=prec)[0]
     xh = host(x, b.shape)
@@ -79,6 +83,26 @@ def test_multi_rhs_multi_kappa_equals_single(cuda, qcu_lib, oracle):
             c.invert(x1, dev(bs[r]), kappa=kappas[r], csw=1.0, tol=1e-10, precision="half")
             x1 = host(x1, bs[r].shape)
             assert np.linalg.norm(xs[r] - x1) / np.linalg.norm(x1) < 1e-8
+
+
+def test_successive_solves_with_different_parameters(cuda, qcu_lib, oracle):
+    """One context, one batch size, solves that differ only in parameters the
+    captured CUDA graphs would bake in (boundary, clover on/off, tolerance):
+    each must solve its own system."""
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 8, 0.4)
+    b = oracle.full_spinor_random(L, 9)
+    cases = [dict(csw=1.0, bc_t=-1.0, tol=1e-10), dict(csw=0.0, bc_t=-1.0, tol=1e-10),
+             dict(csw=1.0, bc_t=1.0, tol=1e-10), dict(csw=1.0, bc_t=-1.0, tol=1e-6)]
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        for kw in cases:
+            x = dev(np.zeros_like(b))
+            rep = c.invert(x, dev(b), kappa=0.13, precision="half", **kw)[0]
+            xh = host(x, b.shape)
+            C = oracle.clover_build(U, L, 0.13 * kw["csw"])
+            res = np.linalg.norm(b - oracle.apply_full(xh, U, C, L, 0.13, kw["bc_t"])) / np.linalg.norm(b)
+            assert rep["converged"] and res < kw["tol"], (kw, rep, res)
 
 
 def test_nan_source_is_rejected(cuda, qcu_lib, oracle):
