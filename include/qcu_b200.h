@@ -154,6 +154,68 @@ int qcuApplyOperator(qcu_context ctx, void* out, const void* in, double kappa, d
 int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, const double* kappas,
               const qcu_solve_params* params, qcu_solve_report* reports);
 
+/* ---- request server: continuous batching over resident configurations ----
+ * No counterpart in the reference (its cg_inverter, src/cg_inverter.cu:260-369,
+ * solves one right-hand side per call). Each registered gauge configuration
+ * becomes resident on first use (gauge field, factored clover bank and a
+ * batch of RHS columns) within a device-memory budget; idle configurations are
+ * evicted to make room. A request (kappa, c_sw, nrhs sources) joins its
+ * configuration's batch as soon as nrhs columns and a clover slot are free,
+ * while the requests already there keep iterating; batches of different
+ * configurations run on their own streams and overlap on the GPU. Sources and
+ * solutions are full AoS spinors, host or device; host buffers should be
+ * pinned (qcuHostAlloc), otherwise the copies block the loop. */
+typedef struct qcu_server_s* qcu_server;
+
+typedef struct {
+  int precision;            /* inner precision (default QCU_PREC_HALF) */
+  double tol;               /* true residual |b - M x|/|b| of every request (1e-10) */
+  int maxiter;              /* per RHS (20000) */
+  double bc_t;              /* time boundary factor (-1) */
+  double delta;             /* reliable-update factor, 0 = default */
+  int columns;              /* RHS columns per resident configuration (16) */
+  int clover_slots;         /* factored clover fields per resident configuration (8) */
+  long long device_budget;  /* device bytes for resident configurations (0 = 85% of free memory) */
+  int autotune;             /* tune launch shapes when a configuration becomes resident (1) */
+} qcu_server_params;
+
+void qcuServerParamsDefault(qcu_server_params* params);
+int qcuServerCreate(qcu_server* server, int device, const qcu_server_params* params);
+/* Waits for the device work of every resident configuration, then frees all. */
+int qcuServerDestroy(qcu_server server);
+/* Registers the seeded synthetic gauge configuration exp(i eps H) (the field
+ * qcuGenerateGauge makes) on this lattice; *config_id names it in requests. */
+int qcuServerAddConfig(qcu_server server, const int lattice[4], unsigned long long seed, double eps, int* config_id);
+/* Makes a configuration resident now (otherwise done by its first request). */
+int qcuServerPrepare(qcu_server server, int config_id);
+/* Queues a solve of M(kappa, c_sw) x_r = b_r, r < nrhs (nrhs <= columns).
+ * Returns at once; *ticket identifies the request. */
+int qcuServerSubmit(qcu_server server, int config_id, double kappa, double csw, int nrhs, const void* b, void* x,
+                    long long* ticket);
+/* One pass of the request loop; never waits for the GPU. *finished receives
+ * the number of requests that completed in this pass. */
+int qcuServerPoll(qcu_server server, int* finished);
+/* *finished = 1 once x holds the solution; then *latency_s is the time from
+ * submission to completion, reports (nrhs entries) are filled and the request's
+ * status is returned. */
+int qcuServerQuery(qcu_server server, long long ticket, int* finished, double* latency_s, qcu_solve_report* reports);
+/* Forgets a finished request. */
+int qcuServerRelease(qcu_server server, long long ticket);
+/* Runs a whole trace: request i is submitted arrival_s[i] seconds (non-
+ * decreasing) after the call starts, and the loop polls until all finished.
+ * latency_s[i] is measured from the scheduled arrival; reports (sum of nrhs
+ * entries, in request order) may be NULL. */
+int qcuServerRunTrace(qcu_server server, int n, const double* arrival_s, const int* config_id, const double* kappa,
+                      const double* csw, const int* nrhs, const void* const* b, void* const* x, double* latency_s,
+                      qcu_solve_report* reports);
+/* Requests submitted and not yet finished. */
+int qcuServerPending(qcu_server server);
+/* Device bytes held by resident configurations. */
+long long qcuServerDeviceBytes(qcu_server server);
+/* Page-locked host memory for sources and solutions (NULL on failure). */
+void* qcuHostAlloc(long long bytes);
+void qcuHostFree(void* p);
+
 /* Times the fused stencil kernel on resident internal fields: `variant`
  * 0 = hop only, 1 = hop + A^-1, 2 = hop + A^-1 + xpay; precision as above;
  * nrhs right-hand sides. Runs `iters` launches and returns the mean device

@@ -58,6 +58,12 @@ class SolveParams(ctypes.Structure):
                 ("delta", ctypes.c_double), ("use_graphs", ctypes.c_int), ("autotune", ctypes.c_int)]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("tol", ctypes.c_double), ("maxiter", ctypes.c_int),
+                ("bc_t", ctypes.c_double), ("delta", ctypes.c_double), ("columns", ctypes.c_int),
+                ("clover_slots", ctypes.c_int), ("device_budget", ctypes.c_longlong), ("autotune", ctypes.c_int)]
+
+
 class SolveReport(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("converged", ctypes.c_int),
                 ("status", ctypes.c_int), ("true_residual", ctypes.c_double), ("kappa", ctypes.c_double)]
@@ -122,6 +128,22 @@ def lib():
             "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
             "qcuDebugFailAllocAfter": (None, [ll]),
             "qcuAutotune": (i, [P, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(d)]),
+            "qcuServerParamsDefault": (None, [ctypes.POINTER(ServerParams)]),
+            "qcuServerCreate": (i, [ctypes.POINTER(P), i, ctypes.POINTER(ServerParams)]),
+            "qcuServerDestroy": (i, [P]),
+            "qcuServerAddConfig": (i, [P, ctypes.POINTER(i), ctypes.c_ulonglong, d, ctypes.POINTER(i)]),
+            "qcuServerPrepare": (i, [P, i]),
+            "qcuServerSubmit": (i, [P, i, d, d, i, P, P, ctypes.POINTER(ll)]),
+            "qcuServerPoll": (i, [P, ctypes.POINTER(i)]),
+            "qcuServerQuery": (i, [P, ll, ctypes.POINTER(i), ctypes.POINTER(d), ctypes.POINTER(SolveReport)]),
+            "qcuServerRelease": (i, [P, ll]),
+            "qcuServerRunTrace": (i, [P, i, ctypes.POINTER(d), ctypes.POINTER(i), ctypes.POINTER(d),
+                                      ctypes.POINTER(d), ctypes.POINTER(i), ctypes.POINTER(P), ctypes.POINTER(P),
+                                      ctypes.POINTER(d), ctypes.POINTER(SolveReport)]),
+            "qcuServerPending": (i, [P]),
+            "qcuServerDeviceBytes": (ll, [P]),
+            "qcuHostAlloc": (P, [ll]),
+            "qcuHostFree": (None, [P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -349,3 +371,141 @@ class Context:
     @property
     def device_bytes(self) -> int:
         return int(lib().qcuContextDeviceBytes(self._h))
+
+
+# ---------------------------------------------------------------------------
+# request server
+# ---------------------------------------------------------------------------
+def server_params(**kw) -> ServerParams:
+    sp = ServerParams()
+    lib().qcuServerParamsDefault(ctypes.byref(sp))
+    for k, v in kw.items():
+        if k == "precision":
+            v = _PREC[v]
+        setattr(sp, k, v)
+    return sp
+
+
+class PinnedBuffer:
+    """Page-locked host memory (qcuHostAlloc) viewed as a numpy complex128 array."""
+
+    def __init__(self, nbytes: int):
+        import numpy as np
+        self.nbytes = int(nbytes)
+        addr = lib().qcuHostAlloc(self.nbytes)
+        if not addr:
+            raise QcuError(QCU_ERR_OUT_OF_MEMORY, f"cannot pin {self.nbytes} host bytes")
+        self.addr = int(addr)
+        buf = (ctypes.c_char * self.nbytes).from_address(self.addr)
+        self.array = np.frombuffer(buf, dtype=np.complex128)
+
+    def free(self):
+        if self.addr:
+            self.array = None
+            lib().qcuHostFree(ctypes.c_void_p(self.addr))
+            self.addr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop over resident gauge configurations
+    (qcuServer* in include/qcu_b200.h)."""
+
+    def __init__(self, device: int = 0, **kw):
+        self._h = ctypes.c_void_p()
+        self.params = server_params(**kw)
+        _check(lib().qcuServerCreate(ctypes.byref(self._h), int(device), ctypes.byref(self.params)))
+        self.lattices = []
+
+    def close(self):
+        if self._h:
+            lib().qcuServerDestroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_config(self, lattice, seed: int, eps: float) -> int:
+        cid = ctypes.c_int(0)
+        L4 = (ctypes.c_int * 4)(*[int(v) for v in lattice])
+        _check(lib().qcuServerAddConfig(self._h, L4, int(seed), float(eps), ctypes.byref(cid)))
+        self.lattices.append(tuple(int(v) for v in lattice))
+        return cid.value
+
+    def prepare(self, config_id: int):
+        _check(lib().qcuServerPrepare(self._h, int(config_id)))
+
+    def submit(self, config_id: int, kappa: float, csw: float, nrhs: int, b, x) -> int:
+        t = ctypes.c_longlong(0)
+        _check(lib().qcuServerSubmit(self._h, int(config_id), float(kappa), float(csw), int(nrhs), _ptr(b), _ptr(x),
+                                     ctypes.byref(t)))
+        return t.value
+
+    def poll(self) -> int:
+        n = ctypes.c_int(0)
+        _check(lib().qcuServerPoll(self._h, ctypes.byref(n)))
+        return n.value
+
+    def query(self, ticket: int, nrhs: int):
+        """(finished, latency_s, reports, status) of a request."""
+        fin, lat = ctypes.c_int(0), ctypes.c_double(0)
+        reps = (SolveReport * nrhs)()
+        code = lib().qcuServerQuery(self._h, int(ticket), ctypes.byref(fin), ctypes.byref(lat), reps)
+        if code == QCU_ERR_INVALID_ARG and not fin.value:
+            _check(code)
+        return bool(fin.value), lat.value, [r.as_dict() for r in reps], code
+
+    def release(self, ticket: int):
+        _check(lib().qcuServerRelease(self._h, int(ticket)))
+
+    def wait(self, ticket: int, nrhs: int, timeout_s: float = 600.0):
+        import time
+        t0 = time.monotonic()
+        while True:
+            fin, lat, reps, code = self.query(ticket, nrhs)
+            if fin:
+                return lat, reps, code
+            if time.monotonic() - t0 > timeout_s:
+                raise QcuError(QCU_ERR_TIMEOUT, f"request {ticket} did not finish in {timeout_s} s")
+            self.poll()
+
+    def run_trace(self, arrival_s, config_id, kappa, csw, nrhs, b, x, raise_on_fail: bool = True):
+        """Runs a timed trace; returns (latency_s list, per-request report lists, status)."""
+        n = len(arrival_s)
+        D = ctypes.c_double * n
+        I = ctypes.c_int * n
+        Pv = ctypes.c_void_p * n
+        lat = D()
+        tot = int(sum(nrhs))
+        reps = (SolveReport * max(tot, 1))()
+        code = lib().qcuServerRunTrace(self._h, n, D(*arrival_s), I(*config_id), D(*kappa), D(*csw), I(*nrhs),
+                                       Pv(*[_ptr(v).value for v in b]), Pv(*[_ptr(v).value for v in x]), lat, reps)
+        if code != QCU_SUCCESS and raise_on_fail:
+            _check(code)
+        out, k = [], 0
+        for m in nrhs:
+            out.append([reps[k + j].as_dict() for j in range(m)])
+            k += m
+        return list(lat), out, code
+
+    @property
+    def pending(self) -> int:
+        return int(lib().qcuServerPending(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().qcuServerDeviceBytes(self._h))

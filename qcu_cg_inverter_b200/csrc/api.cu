@@ -111,9 +111,11 @@ SpinorView Field::view(int parity) const {
   return v;
 }
 
-int Scratch::ensure(const Geom& g, int nrhs, cudaStream_t st) {
-  // partials: one per (rhs, quantity<=2, block); the smallest site tile is 8
-  size_t need = (size_t)((g.Vh_pad * 2 + 7) / 8 + 1) * (size_t)nrhs * 2;
+int Scratch::ensure(const Geom& g, int nrhs, cudaStream_t st, int min_sb) {
+  // partials: one per (rhs, quantity <= 2, block) for up to 2*Vh_pad sites
+  // (full-spinor dot products) in blocks of at least min_sb site lanes
+  if (min_sb < 1) min_sb = 1;
+  size_t need = (size_t)((g.Vh_pad * 2 + min_sb - 1) / min_sb + 1) * (size_t)nrhs * 2;
   if (need > partial_doubles || !partial.p) {
     QCU_CHECK(partial.ensure(need * sizeof(double), st));
     partial_doubles = need;
@@ -459,7 +461,7 @@ int qcuContextCreate(qcu_context* out, const int lattice[4], int device) {
     delete ctx;
     return cuda_status(e, "cudaStreamCreate");
   }
-  int st = ctx->red.ensure(ctx->g, 1, ctx->stream);
+  int st = ctx->red.ensure(ctx->g, 1, ctx->stream, ctx->shape1.Sb);
   if (st != QCU_SUCCESS) {
     delete ctx;
     return st;
@@ -468,7 +470,8 @@ int qcuContextCreate(qcu_context* out, const int lattice[4], int device) {
   return QCU_SUCCESS;
 }
 
-void qcu_solver_workspace_free(qcu_context ctx);  // solver.cu
+extern "C" void qcu_solver_workspace_free(qcu_context ctx);  // engine.cu
+extern "C" long long qcu_engine_device_bytes(qcu_context ctx);
 
 int qcuContextDestroy(qcu_context ctx) {
   clear_error();
@@ -502,6 +505,7 @@ int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes) {
     set_error(QCU_ERR_INVALID_ARG, "block shape must have a power-of-two RHS width <= 32 and 32..256 threads");
     return QCU_ERR_INVALID_ARG;
   }
+  QCU_CHECK(ctx->red.ensure(ctx->g, 1, ctx->stream, site_lanes));
   ctx->shape1 = LaunchShape{rhs_lanes, site_lanes};
   ctx->shape_set = true;
   return QCU_SUCCESS;
@@ -516,7 +520,8 @@ int qcuContextSetHalfOperator(qcu_context ctx, int fast_links) {
 
 long long qcuContextDeviceBytes(qcu_context ctx) {
   if (!ctx) return 0;
-  long long n = ctx->gauge64.bytes + ctx->gauge32.bytes + ctx->gauge16.bytes;
+  long long n = ctx->gauge64.bytes + ctx->gauge32.bytes + ctx->gauge16.bytes + ctx->gauge18.bytes;
+  n += qcu_engine_device_bytes(ctx);
   n += ctx->clover.A64.bytes + ctx->clover.Ainv64.bytes + ctx->clover.Ainv32.bytes + ctx->clover.Ainv16.bytes;
   n += ctx->red.partial.bytes + ctx->lin.data.bytes + ctx->lout.data.bytes + ctx->ltmp.data.bytes +
        ctx->ltmp2.data.bytes + ctx->lx.data.bytes + ctx->stage_in.bytes + ctx->stage_out.bytes;
@@ -832,7 +837,7 @@ static int ref_cg(qcu_context ctx, void* b_vec, void* x_vec, int* iters_out, boo
   QCU_CHECK(spinor_to_internal(ctx, b_vec, b, 2));
   for (Field* f : {&x, &r, &r2, &p, &ap, &tmp, &nb}) QCU_CHECK(f->alloc(PREC_DOUBLE, g.Vh_pad, 1, 2, st));
   const int n = 2 * g.Vh_pad;
-  QCU_CHECK(ctx->red.ensure(g, 1, st));
+  QCU_CHECK(ctx->red.ensure(g, 1, st, ctx->shape1.Sb));
   ReduceArgs red = ctx->red.args();
   double* h = ctx->red.host.as<double>();
   auto dot = [&](const Field& u, const Field& v, double out[2]) -> int {

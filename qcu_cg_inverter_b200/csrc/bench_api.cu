@@ -79,10 +79,10 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   }
   int slot = 0;
   if (variant >= 1) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
-  QCU_CHECK(ctx->red.ensure(g, nrhs, st));
   // the shape the solver would use (tuned when qcuAutotune ran, else the
   // default), unless qcuContextSetShape overrode the single-RHS shape
   LaunchShape sh = (nrhs == 1 && ctx->shape_set) ? ctx->shape1 : ctx_shape(ctx, op, nrhs);
+  QCU_CHECK(ctx->red.ensure(g, nrhs, st, sh.Sb));
   DslashArgs a;
   memset(&a, 0, sizeof(a));
   a.g = g;

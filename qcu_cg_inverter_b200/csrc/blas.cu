@@ -122,6 +122,18 @@ __global__ void __launch_bounds__(256) accumulate_kernel(int nsites, int nrhs, S
   SpinorIO<PL>::store(xlo, s, r, l);
 }
 
+// f = 0 on the RHS in the mask (16-bit fields: norm 0 too)
+template <int P>
+__global__ void __launch_bounds__(256) zero_kernel(int nsites, int nrhs, SpinorView f, const int* active) {
+  typedef typename CompReal<P>::type R;
+  QCU_SITE_RHS
+  if (!valid) return;
+  Spinor<R> z;
+#pragma unroll
+  for (int k = 0; k < 12; k++) z.c[k] = mk(R(0), R(0));
+  SpinorIO<P>::store(f, s, r, z);
+}
+
 // r = b - z (double), |r|^2 (FinNone)
 __global__ void __launch_bounds__(256) residual_kernel(int nsites, int nrhs, SpinorView rv, CSpinorView b, CSpinorView z,
                                                        const int* active, ReduceArgs red) {
@@ -260,6 +272,18 @@ cudaError_t launch_accumulate(int pl, int nsites, int nrhs, SpinorView xhi, Spin
   if (pl == PREC_DOUBLE) accumulate_kernel<PREC_DOUBLE><<<g, b, 0, st>>>(nsites, nrhs, xhi, xlo, active);
   else if (pl == PREC_SINGLE) accumulate_kernel<PREC_SINGLE><<<g, b, 0, st>>>(nsites, nrhs, xhi, xlo, active);
   else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zero(int prec, int nsites, int nrhs, SpinorView f, const int* active, LaunchShape sh,
+                        cudaStream_t st) {
+  dim3 b = blk(sh), g = grd(nsites, nrhs, sh);
+  switch (prec) {
+    case PREC_DOUBLE: zero_kernel<PREC_DOUBLE><<<g, b, 0, st>>>(nsites, nrhs, f, active); break;
+    case PREC_SINGLE: zero_kernel<PREC_SINGLE><<<g, b, 0, st>>>(nsites, nrhs, f, active); break;
+    case PREC_HALF: zero_kernel<PREC_HALF><<<g, b, 0, st>>>(nsites, nrhs, f, active); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

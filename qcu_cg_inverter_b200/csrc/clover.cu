@@ -309,8 +309,9 @@ __global__ void __launch_bounds__(256) clover_apply_kernel(Geom g, int parity, i
   if (valid) {
     Spinor<R> v;
     SpinorIO<P>::load(v, in, s, r);
-    const void* c = clov_idx ? static_cast<const char*>(clov) + clov_stride * (size_t)clov_idx[r] : clov;
-    clover_apply_site<P>(v, c, g.Vh_pad, parity, s);
+    const void* c = clov;
+    if (clov_idx) c = clov_idx[r] >= 0 ? static_cast<const char*>(clov) + clov_stride * (size_t)clov_idx[r] : nullptr;
+    if (c) clover_apply_site<P>(v, c, g.Vh_pad, parity, s);  // negative slot: A = 1
     if (out.data) SpinorIO<P>::store(out, s, r, v);
     if (NORM)
       for (int k = 0; k < 12; k++) nrm += (double)v.c[k].re * v.c[k].re + (double)v.c[k].im * v.c[k].im;

@@ -49,12 +49,15 @@ cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void*
 // spinors: AoS half spinor (12 complex per site) <-> internal, nrhs fields.
 // RHS r of the AoS data starts at aos + r*aos_stride (in complex numbers).
 // ---------------------------------------------------------------------------
+// `count` AoS spinors go to (or come from) RHS columns r0 .. r0+count-1 of the
+// internal field (whose own RHS count is in the view).
 template <int P>
-__global__ void spinor_in_kernel(Geom g, int nrhs, const double2* __restrict__ aos, size_t aos_stride, SpinorView dst) {
+__global__ void spinor_in_kernel(Geom g, int count, const double2* __restrict__ aos, size_t aos_stride, SpinorView dst,
+                                 int r0) {
   typedef typename CompReal<P>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
-  if (s >= g.Vh || r >= nrhs) return;
+  if (s >= g.Vh || r >= count) return;
   const double2* p = aos + r * aos_stride + (size_t)s * 12;
   Spinor<R> v;
 #pragma unroll
@@ -62,43 +65,44 @@ __global__ void spinor_in_kernel(Geom g, int nrhs, const double2* __restrict__ a
     double2 w = p[k];
     v.c[k] = mk((R)w.x, (R)w.y);
   }
-  SpinorIO<P>::store(dst, s, r, v);
+  SpinorIO<P>::store(dst, s, r0 + r, v);
 }
 
 template <int P>
-__global__ void spinor_out_kernel(Geom g, int nrhs, CSpinorView src, double2* __restrict__ aos, size_t aos_stride) {
+__global__ void spinor_out_kernel(Geom g, int count, CSpinorView src, double2* __restrict__ aos, size_t aos_stride,
+                                  int r0) {
   typedef typename CompReal<P>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
-  if (s >= g.Vh || r >= nrhs) return;
+  if (s >= g.Vh || r >= count) return;
   Spinor<R> v;
-  SpinorIO<P>::load(v, src, s, r);
+  SpinorIO<P>::load(v, src, s, r0 + r);
   double2* p = aos + r * aos_stride + (size_t)s * 12;
 #pragma unroll
   for (int k = 0; k < 12; k++) p[k] = make_double2((double)v.c[k].re, (double)v.c[k].im);
 }
 
-cudaError_t launch_spinor_in(int prec, const Geom& g, int nrhs, const void* aos, size_t aos_stride, SpinorView dst,
-                             cudaStream_t st) {
-  dim3 block(1, 128), grid(grid_x(g.Vh, 128), nrhs);
+cudaError_t launch_spinor_in(int prec, const Geom& g, int count, const void* aos, size_t aos_stride, SpinorView dst,
+                             cudaStream_t st, int r0) {
+  dim3 block(1, 128), grid(grid_x(g.Vh, 128), count);
   const double2* a = static_cast<const double2*>(aos);
   switch (prec) {
-    case PREC_DOUBLE: spinor_in_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, nrhs, a, aos_stride, dst); break;
-    case PREC_SINGLE: spinor_in_kernel<PREC_SINGLE><<<grid, block, 0, st>>>(g, nrhs, a, aos_stride, dst); break;
-    case PREC_HALF: spinor_in_kernel<PREC_HALF><<<grid, block, 0, st>>>(g, nrhs, a, aos_stride, dst); break;
+    case PREC_DOUBLE: spinor_in_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, count, a, aos_stride, dst, r0); break;
+    case PREC_SINGLE: spinor_in_kernel<PREC_SINGLE><<<grid, block, 0, st>>>(g, count, a, aos_stride, dst, r0); break;
+    case PREC_HALF: spinor_in_kernel<PREC_HALF><<<grid, block, 0, st>>>(g, count, a, aos_stride, dst, r0); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_spinor_out(int prec, const Geom& g, int nrhs, CSpinorView src, void* aos, size_t aos_stride,
-                              cudaStream_t st) {
-  dim3 block(1, 128), grid(grid_x(g.Vh, 128), nrhs);
+cudaError_t launch_spinor_out(int prec, const Geom& g, int count, CSpinorView src, void* aos, size_t aos_stride,
+                              cudaStream_t st, int r0) {
+  dim3 block(1, 128), grid(grid_x(g.Vh, 128), count);
   double2* a = static_cast<double2*>(aos);
   switch (prec) {
-    case PREC_DOUBLE: spinor_out_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, nrhs, src, a, aos_stride); break;
-    case PREC_SINGLE: spinor_out_kernel<PREC_SINGLE><<<grid, block, 0, st>>>(g, nrhs, src, a, aos_stride); break;
-    case PREC_HALF: spinor_out_kernel<PREC_HALF><<<grid, block, 0, st>>>(g, nrhs, src, a, aos_stride); break;
+    case PREC_DOUBLE: spinor_out_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, count, src, a, aos_stride, r0); break;
+    case PREC_SINGLE: spinor_out_kernel<PREC_SINGLE><<<grid, block, 0, st>>>(g, count, src, a, aos_stride, r0); break;
+    case PREC_HALF: spinor_out_kernel<PREC_HALF><<<grid, block, 0, st>>>(g, count, src, a, aos_stride, r0); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -101,13 +101,14 @@ struct Scratch {
   DevBuf partial, ticket, result;
   PinnedBuf host;
   size_t partial_doubles = 0;
-  int ensure(const Geom& g, int nrhs, cudaStream_t st);
+  // min_sb: the fewest site lanes per block of any launch that reduces
+  int ensure(const Geom& g, int nrhs, cudaStream_t st, int min_sb);
   ReduceArgs args(void* state = nullptr) const {
     return ReduceArgs{partial.as<double>(), ticket.as<unsigned>(), result.as<double>(), state};
   }
 };
 
-struct SolverWorkspace;  // solver.cu
+class Engine;  // engine.cu
 
 }  // namespace qcu
 
@@ -132,7 +133,7 @@ struct qcu_context_s {
   qcu::Field lin, lout, ltmp, ltmp2, lx;
   qcu::DevBuf stage_in, stage_out;  // device staging of host arguments
   qcu::DevBuf status;               // clover build status counters
-  qcu::SolverWorkspace* solver = nullptr;  // owned; freed by qcuContextDestroy (solver.cu)
+  qcu::Engine* engine = nullptr;  // batch engine of qcuInvert; owned, freed by qcuContextDestroy (engine.cu)
   std::map<std::pair<int, int>, qcu::LaunchShape> tuned;  // (precision, nrhs) -> block shape (tune.cu)
   bool tune_cache_loaded = false;
   long long clover_gen = 0;  // bumped whenever the clover bank moves
@@ -164,10 +165,12 @@ bool is_device_ptr(const void* p);
 // kernel launchers (defined in the .cu files)
 cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, void* d18,
                                 cudaStream_t st);
-cudaError_t launch_spinor_in(int prec, const Geom& g, int nrhs, const void* aos, size_t aos_stride, SpinorView dst,
-                             cudaStream_t st);
-cudaError_t launch_spinor_out(int prec, const Geom& g, int nrhs, CSpinorView src, void* aos, size_t aos_stride,
-                              cudaStream_t st);
+// count AoS spinors (RHS r at aos + r*aos_stride complex) <-> RHS columns
+// r0 .. r0+count-1 of an internal field
+cudaError_t launch_spinor_in(int prec, const Geom& g, int count, const void* aos, size_t aos_stride, SpinorView dst,
+                             cudaStream_t st, int r0 = 0);
+cudaError_t launch_spinor_out(int prec, const Geom& g, int count, CSpinorView src, void* aos, size_t aos_stride,
+                              cudaStream_t st, int r0 = 0);
 cudaError_t launch_gauge_random(const Geom& g, uint64_t seed, double eps, void* aos, cudaStream_t st);
 cudaError_t launch_spinor_random(size_t nsites, uint64_t seed, void* aos, cudaStream_t st);
 cudaError_t launch_clover_build(const Geom& g, const void* gauge64, double csw_eff, void* A64, void* Ainv64,
@@ -183,6 +186,8 @@ cudaError_t launch_convert(int pd, int psrc, int nsites, int nrhs, SpinorView ds
                            const ReduceArgs* red, LaunchShape sh, cudaStream_t st);
 cudaError_t launch_accumulate(int pl, int nsites, int nrhs, SpinorView xhi, SpinorView xlo, const int* active,
                               LaunchShape sh, cudaStream_t st);
+cudaError_t launch_zero(int prec, int nsites, int nrhs, SpinorView f, const int* active, LaunchShape sh,
+                        cudaStream_t st);
 cudaError_t launch_residual(int nsites, int nrhs, SpinorView r, CSpinorView b, CSpinorView z, const int* active,
                             const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
 cudaError_t launch_cdot(int prec, int nsites, int nrhs, CSpinorView x, CSpinorView y, const int* active,

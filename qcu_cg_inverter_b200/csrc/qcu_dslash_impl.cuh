@@ -34,19 +34,27 @@ __global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const Dsla
   if (valid) {
     Spinor<R> o;
     hop<PS, PL, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
+    // per-RHS clover slot; a negative slot index means no clover term for
+    // that RHS (A = 1), so Wilson and clover systems can share a batch
     const void* clov = a.clover;
     if (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) {
-      if (a.clover_idx) clov = static_cast<const char*>(a.clover) + a.clover_stride * (size_t)a.clover_idx[r];
+      if (a.clover_idx) {
+        const int ci = a.clover_idx[r];
+        clov = ci >= 0 ? static_cast<const char*>(a.clover) + a.clover_stride * (size_t)ci : nullptr;
+      }
     }
-    if (EPI & EPI_CPRE) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
+    if (EPI & EPI_CPRE)
+      if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     if (EPI & EPI_XPAY) {
       const R c = a.coef ? (R)a.coef[r] : (R)a.coef0;
       Spinor<R> xv;
       SpinorIO<PS>::load(xv, a.x, s, r);
-      if (EPI & EPI_CX) clover_apply_site<PC>(xv, clov, a.g.Vh_pad, a.parity, s);
+      if (EPI & EPI_CX)
+        if (clov) clover_apply_site<PC>(xv, clov, a.g.Vh_pad, a.parity, s);
 #pragma unroll
       for (int k = 0; k < 12; k++) o.c[k] = xv.c[k] + c * o.c[k];
-      if (EPI & EPI_CPOST) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
+      if (EPI & EPI_CPOST)
+        if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     }
     SpinorIO<PS>::store(a.out, s, r, o);
     if (EPI & EPI_NORM) {
@@ -54,7 +62,7 @@ __global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const Dsla
       for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
     }
     if (EPI & EPI_OUT2) {
-      clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
+      if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
       SpinorIO<PS>::store(a.out2, s, r, o);
     }
   }

@@ -76,7 +76,7 @@ int ctx_autotune(qcu_context ctx, int spinor_prec, int nrhs, double* best_ms) {
   }
   int slot;
   QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
-  QCU_CHECK(ctx->red.ensure(g, nrhs, st));
+  QCU_CHECK(ctx->red.ensure(g, nrhs, st, 2));  // smallest candidate: 32 RHS lanes x 2 sites
   DslashArgs a;
   memset(&a, 0, sizeof(a));
   a.g = g;
