@@ -437,6 +437,119 @@ def run_multi(args):
     print(json.dumps(out), flush=True)
 
 
+SERVE_LATTICES = ((8, 8, 8, 8), (16, 16, 16, 32), (24, 24, 24, 48))
+SERVE_WEIGHTS = (0.5, 0.3, 0.2)
+SERVE_RATE = 50.0  # mean arrivals per second (Poisson)
+SERVE_EPS = 0.4  # not fixed by the workload description; recorded in the output
+SERVE_SEED = 2025
+
+
+def serve_trace(n, seed):
+    """n requests: Poisson arrivals (mean 50/s), lattice 8^4 / 16^3x32 / 24^3x48
+    with weights .5/.3/.2, one of 3 gauge configurations per lattice, kappa
+    uniform in [0.120, 0.1375], c_sw in {0, 1}, 1-12 RHS."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    arr = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n))
+    arr -= arr[0]
+    lat = rng.choice(len(SERVE_LATTICES), n, p=SERVE_WEIGHTS)
+    cfg = rng.integers(0, 3, n)
+    kap = rng.uniform(0.120, 0.1375, n)
+    csw = rng.choice([0.0, 1.0], n)
+    nrhs = rng.integers(1, 13, n)
+    return [dict(t=float(arr[i]), lat=int(lat[i]), cfg=int(cfg[i]), kappa=float(kap[i]), csw=float(csw[i]),
+                 nrhs=int(nrhs[i])) for i in range(n)]
+
+
+def run_serve(args):
+    """The serving stream: a seeded Poisson trace run through the request
+    server (continuous batching, one resident batch per gauge configuration).
+    Sources are seeded Gaussian spinors in pinned host memory; solutions are
+    copied back to pinned host memory; latency runs from each request's
+    scheduled arrival to its solution being in host memory."""
+    import numpy as np
+    import torch
+
+    import qcu_cg_inverter_b200 as q
+    device = torch.device("cuda", 0)
+    srv = q.Server(0, columns=args.columns, clover_slots=args.clover_slots, tol=TOL, bc_t=BC_T,
+                   precision=q._PREC[args.precision])
+    cids = {}
+    for li, L in enumerate(SERVE_LATTICES):
+        for c in range(3):
+            cids[(li, c)] = srv.add_config(L, GAUGE_SEED + 1000 * li + c, SERVE_EPS)
+    t_prep = time.time()
+    for cid in cids.values():
+        srv.prepare(cid)
+    t_prep = time.time() - t_prep
+    # pinned pools: 12 Gaussian sources per lattice, and output rings
+    full = [2 * (L[0] * L[1] * L[2] * L[3] // 2) * 12 for L in SERVE_LATTICES]  # complex per full spinor
+    src, out = [], []
+    for li, L in enumerate(SERVE_LATTICES):
+        pb = q.PinnedBuffer(12 * full[li] * 16)
+        with q.Context(L, 0) as c:
+            t = torch.empty(12 * full[li], dtype=torch.complex128, device=device)
+            c.generate_spinor(t, 12, SOURCE_SEED + li)
+            pb.array[:] = t.cpu().numpy()
+            del t
+        src.append(pb)
+        out.append([q.PinnedBuffer(12 * full[li] * 16) for _ in range(args.out_ring)])
+
+    def trace_args(tr):
+        b = [src[r["lat"]].addr for r in tr]
+        x = [out[r["lat"]][i % args.out_ring].addr for i, r in enumerate(tr)]
+        return ([r["t"] for r in tr], [cids[(r["lat"], r["cfg"])] for r in tr], [r["kappa"] for r in tr],
+                [r["csw"] for r in tr], [r["nrhs"] for r in tr], b, x)
+
+    # warm-up trace (other seed): graphs and clover slots of every batch
+    warm = serve_trace(max(args.warmup, 0) * 9, SERVE_SEED + 1)
+    if warm:
+        for r in warm:
+            r["t"] = 0.0
+        srv.run_trace(*trace_args(warm))
+    tr = serve_trace(args.requests, SERVE_SEED)
+    with ClockSampler(0) as clk:
+        clk.start()
+        t0 = time.time()
+        lat, reps, code = srv.run_trace(*trace_args(tr), raise_on_fail=False)
+        wall = time.time() - t0
+        clk.stop()
+    conv = all(r["converged"] for rr in reps for r in rr)
+    nsol = sum(r["nrhs"] for r in tr)
+    lat_ms = sorted(v * 1e3 for v in lat)
+
+    def pct(p):
+        k = min(len(lat_ms) - 1, max(0, int(round(p / 100.0 * (len(lat_ms) - 1)))))
+        return lat_ms[k]
+
+    per_lat = {}
+    for li, L in enumerate(SERVE_LATTICES):
+        v = sorted(lat[i] * 1e3 for i, r in enumerate(tr) if r["lat"] == li)
+        if v:
+            per_lat["x".join(map(str, L))] = {"requests": len(v), "p50_ms": v[len(v) // 2],
+                                              "p99_ms": v[min(len(v) - 1, int(round(0.99 * (len(v) - 1))))]}
+    h2d = sum(r["nrhs"] * full[r["lat"]] * 16 for r in tr)
+    res = {
+        "metric": "serving p50/p99 latency and solves/s (Poisson 50 req/s; 8^4/16^3x32/24^3x48 mix)",
+        "value": nsol / wall, "unit": "RHS solves/s", "requests_per_s": len(tr) / wall,
+        "p50_ms": pct(50), "p99_ms": pct(99), "max_ms": lat_ms[-1], "per_lattice": per_lat,
+        "requests": len(tr), "rhs_solves": nsol, "makespan_s": wall, "arrival_window_s": tr[-1]["t"],
+        "all_converged": conv, "status": code,
+        "max_true_residual": max(r["true_residual"] for rr in reps for r in rr),
+        "iterations_mean": float(np.mean([r["iterations"] for rr in reps for r in rr])),
+        "config": {"workload": "serving stream", "lattices": SERVE_LATTICES, "weights": SERVE_WEIGHTS,
+                   "rate_per_s": SERVE_RATE, "kappa": [0.120, 0.1375], "csw": [0.0, 1.0], "nrhs": [1, 12],
+                   "configs_per_lattice": 3, "eps": SERVE_EPS, "tol": TOL, "precision": args.precision,
+                   "columns_per_config": args.columns, "clover_slots_per_config": args.clover_slots,
+                   "trace_seed": SERVE_SEED, "output_ring_per_lattice": args.out_ring},
+        "e2e": {"h2d_bytes": h2d, "d2h_bytes": h2d},
+        "device_bytes_resident": srv.device_bytes, "prepare_s": t_prep,
+        "clocks": clk.summary(),
+    }
+    srv.close()
+    print(json.dumps(res), flush=True)
+
+
 def run_stencil(args):
     """Times one fused stencil variant alone (Dslash GB/s of the metric), e.g.
     for profiling: --stencil 24 24 24 48 --precision half --variant 2."""
@@ -470,7 +583,15 @@ def main():
     ap.add_argument("--precision", default="half", choices=["half", "single", "double"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="the serving stream through the request server")
+    ap.add_argument("--requests", type=int, default=300, help="--serve: requests in the timed trace")
+    ap.add_argument("--columns", type=int, default=16, help="--serve: RHS columns per resident configuration")
+    ap.add_argument("--clover-slots", type=int, default=8, help="--serve: clover fields per configuration")
+    ap.add_argument("--out-ring", type=int, default=4, help="--serve: pinned output buffers per lattice")
     args = ap.parse_args()
+    if args.serve:
+        run_serve(args)
+        return
     if args.stencil:
         run_stencil(args)
         return

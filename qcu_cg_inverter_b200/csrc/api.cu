@@ -214,7 +214,7 @@ int ctx_clover_reserve(qcu_context ctx, int nslots) {
   return QCU_SUCCESS;
 }
 
-int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot) {
+int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot, bool wait) {
   CloverBank& B = ctx->clover;
   if (!ctx->gauge_loaded) {
     set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
@@ -245,6 +245,12 @@ int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot) {
                                      static_cast<char*>(B.Ainv32.p) + B.b32 * k,
                                      static_cast<char*>(B.Ainv16.p) + B.b16 * k, ctx->status.as<int>(), ctx->stream));
   ctx->launches += 2;
+  if (!wait) {
+    B.csw[k] = csw_eff;
+    B.stamp[k] = ++ctx->clock;
+    *slot = k;
+    return QCU_SUCCESS;
+  }
   int st[2] = {0, 0};
   QCU_CHECK_CUDA(cudaMemcpyAsync(st, ctx->status.p, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
   QCU_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -255,6 +261,15 @@ int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot) {
   B.csw[k] = csw_eff;
   B.stamp[k] = ++ctx->clock;
   *slot = k;
+  return QCU_SUCCESS;
+}
+
+int ctx_set_stream_priority(qcu_context ctx, int priority) {
+  QCU_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  cudaStream_t s = nullptr;
+  QCU_CHECK_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+  cudaStreamDestroy(ctx->stream);
+  ctx->stream = s;
   return QCU_SUCCESS;
 }
 

@@ -39,15 +39,21 @@ template <class R> QCU_HD Cplx<R> conj(Cplx<R> a) { return {a.re, -a.im}; }
 template <class R> QCU_HD Cplx<R> mul_i(Cplx<R> a) { return {-a.im, a.re}; }  // i*a
 template <class R> QCU_HD Cplx<R>& operator+=(Cplx<R>& a, Cplx<R> b) { a.re += b.re; a.im += b.im; return a; }
 template <class R> QCU_HD Cplx<R>& operator-=(Cplx<R>& a, Cplx<R> b) { a.re -= b.re; a.im -= b.im; return a; }
-// a += b*c
+// a += b*c, as four fused multiply-adds into the accumulator (written as
+// a + (x - y) the compiler may not reassociate, and emits a multiply, an FMA
+// and an add per component)
 template <class R> QCU_HD void cmac(Cplx<R>& a, Cplx<R> b, Cplx<R> c) {
-  a.re += b.re * c.re - b.im * c.im;
-  a.im += b.re * c.im + b.im * c.re;
+  a.re = fma(b.re, c.re, a.re);
+  a.re = fma(-b.im, c.im, a.re);
+  a.im = fma(b.re, c.im, a.im);
+  a.im = fma(b.im, c.re, a.im);
 }
 // a += conj(b)*c
 template <class R> QCU_HD void cmac_conj(Cplx<R>& a, Cplx<R> b, Cplx<R> c) {
-  a.re += b.re * c.re + b.im * c.im;
-  a.im += b.re * c.im - b.im * c.re;
+  a.re = fma(b.re, c.re, a.re);
+  a.re = fma(b.im, c.im, a.re);
+  a.im = fma(b.re, c.im, a.im);
+  a.im = fma(-b.im, c.re, a.im);
 }
 
 template <class R> struct Spinor {

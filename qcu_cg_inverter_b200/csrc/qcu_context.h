@@ -146,7 +146,12 @@ namespace qcu {
 // context helpers (api.cu). `op` arguments are OpVariant values (PREC_*
 // values are the matching uniform variants).
 int ctx_check(qcu_context ctx);
-int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot);  // builds on demand
+// Builds on demand. wait = false enqueues the build without reading back its
+// pivot check (a singular block then shows up as a breakdown of the solve).
+int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot, bool wait = true);
+// Replaces the context's stream by one with this scheduling priority
+// (cudaDeviceGetStreamPriorityRange); only while no work is queued on it.
+int ctx_set_stream_priority(qcu_context ctx, int priority);
 int ctx_clover_reserve(qcu_context ctx, int nslots);
 const void* ctx_clover_ptr(qcu_context ctx, int op, bool inverse);
 size_t ctx_clover_stride(qcu_context ctx, int op);

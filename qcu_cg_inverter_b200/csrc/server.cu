@@ -18,6 +18,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <deque>
 #include <map>
@@ -27,6 +28,8 @@
 #include "qcu_engine.h"
 
 using namespace qcu;
+
+extern "C" void qcu_solver_workspace_free(qcu_context ctx);  // engine.cu
 
 namespace {
 
@@ -96,14 +99,40 @@ long long resident_bytes(const qcu_server_s* s) {
   return n;
 }
 
+// frees a context without touching the error channel (qcuContextDestroy
+// clears it, which would lose the cause of a failed setup)
+void destroy_context(qcu_context ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  qcu_solver_workspace_free(ctx);
+  delete ctx;
+}
+
 void evict(Resident& R) {
   R.eng.reset();
-  if (R.ctx) qcuContextDestroy(R.ctx);
+  destroy_context(R.ctx);
   R.ctx = nullptr;
   R.bytes = 0;
 }
 
 bool busy(const Resident& R) { return R.eng && !R.eng->idle(); }
+
+long long volume(const int L[4]) { return (long long)L[0] * L[1] * L[2] * L[3]; }
+
+// rank of this lattice among the distinct registered volumes (smallest =
+// greatest priority), clamped to the device's priority range
+int priority_for(const qcu_server_s* s, const Resident& R) {
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  std::vector<long long> vols;
+  for (const Resident& C : s->configs)
+    if (std::find(vols.begin(), vols.end(), volume(C.L)) == vols.end()) vols.push_back(volume(C.L));
+  std::sort(vols.begin(), vols.end());
+  const int rank = (int)(std::find(vols.begin(), vols.end(), volume(R.L)) - vols.begin());
+  const int p = greatest + rank;  // greatest is the numerically smallest
+  return p > least ? least : p;
+}
 
 int make_resident(qcu_server_s* s, int id) {
   Resident& R = s->configs[id];
@@ -120,7 +149,11 @@ int make_resident(qcu_server_s* s, int id) {
   }
   qcu_context ctx = nullptr;
   QCU_CHECK(qcuContextCreate(&ctx, R.L, s->device));
-  int st = qcuGenerateGauge(ctx, R.seed, R.eps);
+  // smaller lattices get higher stream priority: their short kernels are
+  // scheduled as soon as SMs free up instead of queueing behind the blocks of
+  // large-lattice batches
+  int st = ctx_set_stream_priority(ctx, priority_for(s, R));
+  if (st == QCU_SUCCESS) st = qcuGenerateGauge(ctx, R.seed, R.eps);
   if (st == QCU_SUCCESS) st = ctx_clover_reserve(ctx, s->P.clover_slots);
   if (st == QCU_SUCCESS && s->P.autotune && !ctx_is_tuned(ctx, ctx_op(ctx, s->P.precision), s->P.columns))
     st = ctx_autotune(ctx, s->P.precision, s->P.columns, nullptr);
@@ -136,10 +169,13 @@ int make_resident(qcu_server_s* s, int id) {
     ep.graphs = true;
     st = eng->configure(ctx, s->P.columns, ep);
   }
-  if (st == QCU_SUCCESS) st = cuda_status(cudaStreamSynchronize(ctx->stream), "resident setup");
+  if (st == QCU_SUCCESS) {
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "resident setup");
+  }
   if (st != QCU_SUCCESS) {
     eng.reset();
-    qcuContextDestroy(ctx);
+    destroy_context(ctx);
     return st;
   }
   R.ctx = ctx;
@@ -175,7 +211,7 @@ int try_admit(qcu_server_s* s, Request* q) {
       best = run > best ? run : best;
     }
     if (best < q->nrhs) return QCU_ERR_BUSY;
-    QCU_CHECK(ctx_clover_slot(R.ctx, csw_eff, &q->group.cidx));
+    QCU_CHECK(ctx_clover_slot(R.ctx, csw_eff, &q->group.cidx, false));
   }
   st = E.admit(&q->group);
   if (st != QCU_SUCCESS) return st;
