@@ -42,6 +42,10 @@ LATTICE = (16, 16, 16, 32)
 KAPPA, CSW, EPS, BC_T, TOL = 0.1375, 1.0, 0.4, -1.0, 1e-10
 GAUGE_SEED, SOURCE_SEED = 20241, 7
 ROOF_LATTICE = (32, 32, 32, 64)
+# DRAM bytes (read + write) per output site of the fused 16-bit stencil,
+# from an ncu capture of one launch at 32^4 (592.7 MB for 524288 sites);
+# the traffic grows with the number of sites, so a 32^3x64 launch moves twice that
+ROOF_TRAFFIC_BYTES_PER_SITE = 592.7e6 / 524288
 METRIC = "CG time to |r|/|b|<1e-10, mixed vs FP64 (16^3x32 Wilson-clover, kappa 0.1375, c_sw 1)"
 
 
@@ -254,6 +258,7 @@ def run_ours(args, world, rank, local):
         # dominant kernel: the fused 16-bit stencil (hop + A^-1 + xpay + second output + norm)
         hbm, src = peaks()
         roof = q.Context(ROOF_LATTICE, local)
+        V_roof = roof.volume
         roof.generate_gauge(GAUGE_SEED, 0.5)
         for p in ("half", "double"):
             roof.autotune(p, 1)
@@ -283,7 +288,10 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": world * steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": V * 12 * 16,
                     "d2h_bytes_per_step": V * 12 * 16},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_source": src, "traffic": None,
+                         "peak_source": src,
+                         "traffic": ROOF_TRAFFIC_BYTES_PER_SITE * (V_roof // 2),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                                           "32^4, scaled by the site count",
                          "kernel": "dslash half hop+A^-1+xpay+out2+norm, 32^3x64, 1 RHS",
                          "bytes_per_launch": nbytes, "ms_per_launch": ms},
             "dslash": {"lattice": ROOF_LATTICE,
