@@ -202,7 +202,7 @@ def run_ours(args, world, rank, local):
     x = torch.zeros_like(b)
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
-    kw = dict(kappa=KAPPA, csw=CSW, bc_t=BC_T, tol=TOL)
+    kw = dict(kappa=KAPPA, csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta)
 
     def solve(xx, bb, prec):
         rep = ctx.invert(xx, bb, precision=prec, **kw)[0]
@@ -401,7 +401,7 @@ def run_multi(args):
     b = src12.repeat(len(MULTI_KAPPAS), 1).contiguous()
     kap = [k for k in MULTI_KAPPAS for _ in range(12)]
     x = torch.zeros_like(b)
-    kw = dict(csw=CSW, bc_t=BC_T, tol=TOL)
+    kw = dict(csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta)
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
 
     def timed(fn):
@@ -567,7 +567,7 @@ def run_stencil(args):
         c.generate_gauge(GAUGE_SEED, 0.5)
         if args.sb:
             c.set_shape(1, args.sb)
-        else:
+        elif not args.no_autotune:  # else: the shape from QCU_TUNE_CACHE or the default
             c.autotune(args.precision, args.nrhs)
         ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
     gbs = nbytes / (ms / 1e3) / 1e9
@@ -584,6 +584,7 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--sb", type=int, default=0, help="site lanes per block for --stencil (0 = library default)")
+    ap.add_argument("--no-autotune", action="store_true", help="--stencil: keep the cached or default shape")
     ap.add_argument("--multi", action="store_true", help="the 48-RHS 24^3x48 batch against FP64 single-RHS")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -591,6 +592,7 @@ def main():
     ap.add_argument("--precision", default="half", choices=["half", "single", "double"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--delta", type=float, default=0.0, help="reliable-update factor (0 = library default)")
     ap.add_argument("--serve", action="store_true", help="the serving stream through the request server")
     ap.add_argument("--requests", type=int, default=300, help="--serve: requests in the timed trace")
     ap.add_argument("--columns", type=int, default=16, help="--serve: RHS columns per resident configuration")

@@ -261,6 +261,7 @@ cudaError_t launch_convert(int pd, int psrc, int nsites, int nrhs, SpinorView ds
   else if (pd == PREC_DOUBLE && psrc == PREC_SINGLE) { QCU_CV(PREC_DOUBLE, PREC_SINGLE) }
   else if (pd == PREC_DOUBLE && psrc == PREC_HALF) { QCU_CV(PREC_DOUBLE, PREC_HALF) }
   else if (pd == PREC_HALF && psrc == PREC_HALF) { QCU_CV(PREC_HALF, PREC_HALF) }
+  else if (pd == PREC_SINGLE && psrc == PREC_HALF) { QCU_CV(PREC_SINGLE, PREC_HALF) }
   else return cudaErrorInvalidValue;
 #undef QCU_CV
   return cudaGetLastError();

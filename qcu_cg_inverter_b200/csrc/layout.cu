@@ -50,7 +50,9 @@ cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void*
 // RHS r of the AoS data starts at aos + r*aos_stride (in complex numbers).
 // ---------------------------------------------------------------------------
 // `count` AoS spinors go to (or come from) RHS columns r0 .. r0+count-1 of the
-// internal field (whose own RHS count is in the view).
+// internal field (whose own RHS count is in the view). Threads run over RHS
+// first (threadIdx.x) and sites second, as in the solver kernels, so the
+// internal side of a warp is a contiguous run of 16-byte chunks.
 template <int P>
 __global__ void spinor_in_kernel(Geom g, int count, const double2* __restrict__ aos, size_t aos_stride, SpinorView dst,
                                  int r0) {
@@ -82,9 +84,18 @@ __global__ void spinor_out_kernel(Geom g, int count, CSpinorView src, double2* _
   for (int k = 0; k < 12; k++) p[k] = make_double2((double)v.c[k].re, (double)v.c[k].im);
 }
 
+// 128 threads: up to 16 RHS lanes (the smallest power of two >= count) x sites
+static void layout_shape(const Geom& g, int count, dim3* grid, dim3* block) {
+  int rb = 1;
+  while (rb < count && rb < 16) rb *= 2;
+  *block = dim3(rb, 128 / rb);
+  *grid = dim3(grid_x(g.Vh, 128 / rb), (count + rb - 1) / rb);
+}
+
 cudaError_t launch_spinor_in(int prec, const Geom& g, int count, const void* aos, size_t aos_stride, SpinorView dst,
                              cudaStream_t st, int r0) {
-  dim3 block(1, 128), grid(grid_x(g.Vh, 128), count);
+  dim3 block, grid;
+  layout_shape(g, count, &grid, &block);
   const double2* a = static_cast<const double2*>(aos);
   switch (prec) {
     case PREC_DOUBLE: spinor_in_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, count, a, aos_stride, dst, r0); break;
@@ -97,7 +108,8 @@ cudaError_t launch_spinor_in(int prec, const Geom& g, int count, const void* aos
 
 cudaError_t launch_spinor_out(int prec, const Geom& g, int count, CSpinorView src, void* aos, size_t aos_stride,
                               cudaStream_t st, int r0) {
-  dim3 block(1, 128), grid(grid_x(g.Vh, 128), count);
+  dim3 block, grid;
+  layout_shape(g, count, &grid, &block);
   double2* a = static_cast<double2*>(aos);
   switch (prec) {
     case PREC_DOUBLE: spinor_out_kernel<PREC_DOUBLE><<<grid, block, 0, st>>>(g, count, src, a, aos_stride, r0); break;

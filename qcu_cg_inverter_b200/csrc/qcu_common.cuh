@@ -73,12 +73,39 @@ template <class R> QCU_HD void su3_reconstruct(Link<R>& L) {
 // ---------------------------------------------------------------------------
 // lattice geometry
 // ---------------------------------------------------------------------------
+// Division by a lattice extent d without a division instruction (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994):
+// with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (umulhi(m, n) + n) >> l for every 0 <= n < 2^31.
+struct FastDiv {
+  unsigned m;
+  int l, d;
+};
+inline FastDiv make_fastdiv(int d) {
+  FastDiv f;
+  int l = 0;
+  while ((1ll << l) < d) l++;
+  f.l = l;
+  f.d = d;
+  f.m = (unsigned)((((unsigned long long)1 << 32) * (((unsigned long long)1 << l) - (unsigned long long)d)) /
+                       (unsigned long long)d + 1);
+  return f;
+}
+QCU_HD int fdiv(int n, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
+  return (int)((__umulhi(f.m, (unsigned)n) + (unsigned)n) >> f.l);
+#else
+  return n / f.d;
+#endif
+}
+
 struct Geom {
   int Lx, Ly, Lz, Lt;
   int Lxh;      // Lx/2
   int Vh;       // sites per parity
   int Vh_pad;   // Vh rounded up to the 32-site block
   int sy, sz, st;  // checkerboard strides of y, z, t: Lxh, Lxh*Ly, Lxh*Ly*Lz
+  FastDiv dxh, dy, dz;  // division by Lxh, Ly, Lz
 };
 
 inline Geom make_geom(const int L[4]) {
@@ -90,6 +117,9 @@ inline Geom make_geom(const int L[4]) {
   g.sy = g.Lxh;
   g.sz = g.Lxh * g.Ly;
   g.st = g.Lxh * g.Ly * g.Lz;
+  g.dxh = make_fastdiv(g.Lxh);
+  g.dy = make_fastdiv(g.Ly);
+  g.dz = make_fastdiv(g.Lz);
   return g;
 }
 
@@ -104,12 +134,12 @@ struct Nbrs {
 
 QCU_HD Nbrs neighbours(const Geom& g, int s, int parity) {
   Nbrs n;
-  int xh = s % g.Lxh;
-  int r = s / g.Lxh;
-  int y = r % g.Ly;
-  r /= g.Ly;
-  int z = r % g.Lz;
-  int t = r / g.Lz;
+  int r = fdiv(s, g.dxh);
+  const int xh = s - r * g.Lxh;
+  const int r2 = fdiv(r, g.dy);
+  const int y = r - r2 * g.Ly;
+  const int t = fdiv(r2, g.dz);
+  const int z = r2 - t * g.Lz;
   n.t = t;
   int eo = (y + z + t) & 1;
   int xf = (eo != parity) ? (xh + 1 == g.Lxh ? 0 : xh + 1) : xh;

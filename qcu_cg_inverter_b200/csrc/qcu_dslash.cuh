@@ -139,9 +139,182 @@ QCU_D void hop_dir(Spinor<R>& o, const Geom& g, const Nbrs& nb, int parity, int 
   reconstruct<MU, false, F>(o, a, b);
 }
 
+// ---------------------------------------------------------------------------
+// 16-bit spinors: the hop in paired FP32 instructions (sm_100 FFMA2/FADD2/
+// FMUL2). Two-component spin vectors are kept "spin-paired": lane 0 holds the
+// upper component (h0, or spin 0 / spin 2 of the output), lane 1 the lower
+// (h1, or spin 1 / spin 3), with real and imaginary parts in separate pairs.
+// One SU(3) multiply then serves both half-spinor components, and the
+// projection, scaling and reconstruction act on two components per
+// instruction. The 16-bit decode writes the neighbour's components straight
+// into the pairs each direction needs. Same arithmetic as the scalar path per
+// component (sums may associate differently).
+// ---------------------------------------------------------------------------
+struct HalfPair {
+  float2 re[3], im[3];
+};
+
+// Spin-paired accumulator: U = (o0, o1), L = (o2, o3), X = (o3, o2) (the
+// directions whose reconstruction pairs the lower spins in swapped order add
+// into X; L and X are combined once at the end).
+struct SpinPair {
+  float2 ure[3], uim[3], lre[3], lim[3], xre[3], xim[3];
+};
+
+// integer-valued 16-bit components of words a and b as a pair (offset removed
+// by one paired add)
+QCU_D float2 dec_lo2(int a, int b) {
+  return fadd2(make_float2(u16f(a, 0x7410), u16f(b, 0x7410)), splat2(-8421376.0f));
+}
+QCU_D float2 dec_hi2(int a, int b) {
+  return fadd2(make_float2(u16f(a, 0x7432), u16f(b, 0x7432)), splat2(-8421376.0f));
+}
+QCU_D int word_of(const int4 w[3], int k) {
+  const int4 c = w[k >> 2];
+  const int l = k & 3;
+  return l == 0 ? c.x : (l == 1 ? c.y : (l == 2 ? c.z : c.w));
+}
+
+// h = P_mu psi of the 16-bit neighbour spinor, spin-paired and scaled by its
+// norm times `phase`. Same projector rows as project().
+template <int MU, bool FWD, int F>
+QCU_D void load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, float phase) {
+  constexpr int S = FWD ? -F : F;
+  constexpr float fS = (float)S;
+  constexpr bool SWAP = (MU == 0 || MU == 1);  // lower pair as (p3, p2)
+  const int4* p = static_cast<const int4*>(in.data);
+  int4 w[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) w[c] = p[chunk_index(c, s, r, 3, in.nrhs)];
+  const float nm = in.norm[(size_t)s * in.nrhs + r] * kInvFix * phase;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    // component k = 3*spin + colour; word k holds (re, im) as (lo, hi)
+    const int w0 = word_of(w, c), w1 = word_of(w, 3 + c);
+    const int w2 = word_of(w, SWAP ? 9 + c : 6 + c), w3 = word_of(w, SWAP ? 6 + c : 9 + c);
+    const float2 Pre = dec_lo2(w0, w1), Pim = dec_hi2(w0, w1);
+    const float2 Qre = dec_lo2(w2, w3), Qim = dec_hi2(w2, w3);
+    float2 hre, him;
+    if constexpr (MU == 0) {  // h0 = p0 + S i p3, h1 = p1 + S i p2; Q = (p3, p2)
+      hre = ffma2(Qim, splat2(-fS), Pre);
+      him = ffma2(Qre, splat2(fS), Pim);
+    } else if constexpr (MU == 1) {  // h0 = p0 - S p3, h1 = p1 + S p2; Q = (p3, p2)
+      hre = ffma2(Qre, make_float2(-fS, fS), Pre);
+      him = ffma2(Qim, make_float2(-fS, fS), Pim);
+    } else if constexpr (MU == 2) {  // h0 = p0 + S i p2, h1 = p1 - S i p3; Q = (p2, p3)
+      hre = ffma2(Qim, make_float2(-fS, fS), Pre);
+      him = ffma2(Qre, make_float2(fS, -fS), Pim);
+    } else {  // h0 = p0 + S p2, h1 = p1 + S p3; Q = (p2, p3)
+      hre = ffma2(Qre, splat2(fS), Pre);
+      him = ffma2(Qim, splat2(fS), Pim);
+    }
+    h.re[c] = fmul2(hre, splat2(nm));
+    h.im[c] = fmul2(him, splat2(nm));
+  }
+}
+
+// a = U h (FWD) or U^dag h, both spin components at once
+template <bool FWD>
+QCU_D void su3_mul_pair(HalfPair& a, const Link<float>& U, const HalfPair& h) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    float2 re = make_float2(0.f, 0.f), im = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const Cplx<float> u = FWD ? U.u[i * 3 + j] : U.u[j * 3 + i];
+      const float2 ur = splat2(u.re), ui = splat2(u.im);
+      if (FWD) {  // u h
+        re = ffma2(ur, h.re[j], re);
+        re = ffma2(fneg2(ui), h.im[j], re);
+        im = ffma2(ur, h.im[j], im);
+        im = ffma2(ui, h.re[j], im);
+      } else {  // conj(u) h
+        re = ffma2(ur, h.re[j], re);
+        re = ffma2(ui, h.im[j], re);
+        im = ffma2(ur, h.im[j], im);
+        im = ffma2(fneg2(ui), h.re[j], im);
+      }
+    }
+    a.re[i] = re;
+    a.im[i] = im;
+  }
+}
+
+// out += reconstruct(a), a spin-paired (lanes: U h0, U h1); same rows as reconstruct()
+template <int MU, bool FWD, int F>
+QCU_D void reconstruct_pair(SpinPair& o, const HalfPair& a) {
+  constexpr int S = FWD ? -F : F;
+  constexpr float fS = (float)S;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.ure[c] = fadd2(o.ure[c], a.re[c]);
+    o.uim[c] = fadd2(o.uim[c], a.im[c]);
+    if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a  ->  X = (o3, o2) -= S i (a, b)
+      o.xre[c] = ffma2(a.im[c], splat2(fS), o.xre[c]);
+      o.xim[c] = ffma2(a.re[c], splat2(-fS), o.xim[c]);
+    } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a  ->  X += (-S a, S b)
+      o.xre[c] = ffma2(a.re[c], make_float2(-fS, fS), o.xre[c]);
+      o.xim[c] = ffma2(a.im[c], make_float2(-fS, fS), o.xim[c]);
+    } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b  ->  L += (-S i a, S i b)
+      o.lre[c] = ffma2(a.im[c], make_float2(fS, -fS), o.lre[c]);
+      o.lim[c] = ffma2(a.re[c], make_float2(-fS, fS), o.lim[c]);
+    } else {  // o2 += S a, o3 += S b
+      o.lre[c] = ffma2(a.re[c], splat2(fS), o.lre[c]);
+      o.lim[c] = ffma2(a.im[c], splat2(fS), o.lim[c]);
+    }
+  }
+}
+
+template <int PL, int MU, int F>
+QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, int s, int r, const CSpinorView& in,
+                        const void* gauge, float bc_t) {
+  Link<float> U;
+  HalfPair h, a;
+  LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
+  load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
+  su3_mul_pair<true>(a, U, h);
+  reconstruct_pair<MU, true, F>(o, a);
+  LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
+  load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
+  su3_mul_pair<false>(a, U, h);
+  reconstruct_pair<MU, false, F>(o, a);
+}
+
+template <int PL, bool DAG>
+QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, int r, const CSpinorView& in,
+                         const void* gauge, float bc_t) {
+  constexpr int F = DAG ? -1 : 1;
+  SpinPair o;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.ure[c] = o.uim[c] = o.lre[c] = o.lim[c] = o.xre[c] = o.xim[c] = make_float2(0.f, 0.f);
+  }
+  const Nbrs nb = neighbours(g, s, parity);
+  hop_dir_pair<PL, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir_pair<PL, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir_pair<PL, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir_pair<PL, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    out.c[c] = mk(o.ure[c].x, o.uim[c].x);
+    out.c[3 + c] = mk(o.ure[c].y, o.uim[c].y);
+    out.c[6 + c] = mk(o.lre[c].x + o.xre[c].y, o.lim[c].x + o.xim[c].y);
+    out.c[9 + c] = mk(o.lre[c].y + o.xre[c].x, o.lim[c].y + o.xim[c].x);
+  }
+}
+
 template <int PS, int PL, bool DAG, class R>
 QCU_D void hop(Spinor<R>& o, const Geom& g, int parity, int s, int r, const CSpinorView& in,
                const void* gauge, R bc_t) {
+// Paired-FP32 hop for 16-bit spinors (1, default) or the scalar one (0).
+// Measured on B200 at 32^4 with 16 RHS: hop 677 vs 733 us.
+#ifndef QCU_HOP_FFMA2
+#define QCU_HOP_FFMA2 1
+#endif
+  if constexpr (PS == PREC_HALF && QCU_HOP_FFMA2) {
+    hop_half_pair<PL, DAG>(o, g, parity, s, r, in, gauge, bc_t);
+    return;
+  }
   constexpr int F = DAG ? -1 : 1;
 #pragma unroll
   for (int k = 0; k < 12; k++) o.c[k] = mk(R(0), R(0));

@@ -21,10 +21,20 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_MINB
 #define QCU_DSLASH_MINB 2
 #endif
+// The 16-bit kernel with the second clover output (the CG's fused Mhat half
+// step) gets an 85-register cap instead: measured at 32^4, 16 RHS: 1246 vs
+// 1348 us (24 instead of 16 resident warps; 36 bytes of spills), while the
+// other 16-bit kernels are faster at 128 registers (hop: 677 vs 742 us).
+#ifndef QCU_DSLASH_MINB16_OUT2
+#define QCU_DSLASH_MINB16_OUT2 3
+#endif
+constexpr int dslash_minb(int op, int epi) {
+  return (op_spinor_prec(op) == PREC_HALF && (epi & EPI_OUT2)) ? QCU_DSLASH_MINB16_OUT2 : QCU_DSLASH_MINB;
+}
 
 // OP selects the storage of spinors, links and clover (OpVariant).
 template <int OP, bool DAG, int EPI, class Fin>
-__global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const DslashArgs a) {
+__global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const DslashArgs a) {
   constexpr int PS = op_spinor_prec(OP), PL = op_link_format(OP), PC = op_clover_prec(OP);
   typedef typename CompReal<PS>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
@@ -56,17 +66,40 @@ __global__ void __launch_bounds__(256, QCU_DSLASH_MINB) dslash_kernel(const Dsla
       if (EPI & EPI_CPOST)
         if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     }
-    SpinorIO<PS>::store(a.out, s, r, o);
-    if (EPI & EPI_NORM) {
+    if constexpr ((EPI & EPI_CGXR) != 0) {
+      // x += alpha p, r -= alpha out (the out of this kernel is the CG's z)
+      constexpr int PA = PS == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE;
+      typedef typename CompReal<PA>::type RA;
+      const RA al = (RA)a.alpha[r];
+      Spinor<RA> xv, rv;
+      Spinor<R> pv;
+      SpinorIO<PA>::load(xv, a.xacc, s, r);
+      SpinorIO<PA>::load(rv, a.racc, s, r);
+      SpinorIO<PS>::load(pv, a.pvec, s, r);
 #pragma unroll
-      for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
+      for (int k = 0; k < 12; k++) {
+        xv.c[k].re += al * (RA)pv.c[k].re;
+        xv.c[k].im += al * (RA)pv.c[k].im;
+        rv.c[k].re -= al * (RA)o.c[k].re;
+        rv.c[k].im -= al * (RA)o.c[k].im;
+      }
+      SpinorIO<PA>::store(a.xacc, s, r, xv);
+      SpinorIO<PA>::store(a.racc, s, r, rv);
+#pragma unroll
+      for (int k = 0; k < 12; k++) nrm += (double)rv.c[k].re * rv.c[k].re + (double)rv.c[k].im * rv.c[k].im;
+    } else {
+      SpinorIO<PS>::store(a.out, s, r, o);
+      if (EPI & EPI_NORM) {
+#pragma unroll
+        for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
+      }
     }
     if (EPI & EPI_OUT2) {
       if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
       SpinorIO<PS>::store(a.out2, s, r, o);
     }
   }
-  if (EPI & EPI_NORM) {
+  if (EPI & (EPI_NORM | EPI_CGXR)) {
     double v[1] = {nrm};
     block_reduce_finish<1, Fin>(v, a.nrhs, a.red);
   }
@@ -76,11 +109,14 @@ template <int P, bool DAG>
 static DslashKernelFn pick(int epi, int fin) {
 #define QCU_CASE(E)                                                                     \
   case (E):                                                                             \
-    if ((E)&EPI_NORM) {                                                                 \
+    if constexpr (((E)&EPI_CGXR) != 0) {                                                \
+      return fin == FIN_CG_BETA ? dslash_kernel<P, DAG, (E), FinCgBeta> : nullptr;      \
+    } else if constexpr (((E)&EPI_NORM) != 0) {                                         \
       if (fin == FIN_CG_ALPHA) return dslash_kernel<P, DAG, (E), FinCgAlpha>;           \
       return dslash_kernel<P, DAG, (E), FinNone>;                                       \
-    }                                                                                   \
-    return dslash_kernel<P, DAG, (E), FinNone>;
+    } else {                                                                            \
+      return dslash_kernel<P, DAG, (E), FinNone>;                                       \
+    }
   switch (epi) {
     QCU_CASE(0)
     QCU_CASE(EPI_CPRE)
@@ -92,6 +128,7 @@ static DslashKernelFn pick(int epi, int fin) {
     QCU_CASE(EPI_CPRE | EPI_XPAY | EPI_OUT2)
     QCU_CASE(EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM)
     QCU_CASE(EPI_XPAY | EPI_NORM)
+    QCU_CASE(EPI_XPAY | EPI_CGXR)
     default:
       return nullptr;
   }

@@ -61,17 +61,18 @@ template <> struct SpinorIO<PREC_SINGLE> {
 };
 
 // 16-bit fixed point <-> float without the conversion unit (I2F/F2I issue on
-// the quarter-rate XU pipe, which bounded the 16-bit stencil): a two's
-// complement v in [-32768, 32767], sign-flipped to v + 32768, is placed in the
-// mantissa of 2^23 (0x4B000000), so the float equals 2^23 + 32768 + v and one
-// exact subtraction recovers v. Encoding adds 1.5*2^23, which rounds to the
-// nearest integer (ties to even, as __float2int_rn) and leaves that integer's
-// two's complement in the low 16 bits of the float.
-QCU_D float lo16(int w) { return __uint_as_float(((unsigned)w & 0xffffu) ^ 0x4B008000u) - 8421376.0f; }
-QCU_D float hi16(int w) { return __uint_as_float(((unsigned)w >> 16) ^ 0x4B008000u) - 8421376.0f; }
-QCU_D int pack16(float a, float b) {  // |a|, |b| <= 32767.5
-  unsigned ia = __float_as_uint(a + 12582912.0f);
-  unsigned ib = __float_as_uint(b + 12582912.0f);
+// the quarter-rate XU pipe, which bounded the 16-bit stencil). A value v in
+// [-32768, 32767] is stored offset-binary, as u = v + 32768. Decoding places u
+// in the mantissa of 2^23 with one byte permute (bytes u.lo, u.hi, 0x00, 0x4B),
+// so the float equals 2^23 + 32768 + v and one exact subtraction recovers v.
+// Encoding adds 2^23 + 32768, which rounds to the nearest integer (ties to
+// even, as __float2int_rn) and leaves u in the low 16 bits of the float.
+QCU_D float u16f(int w, unsigned sel) { return __uint_as_float(__byte_perm((unsigned)w, 0x4B000000u, sel)); }
+QCU_D float lo16(int w) { return u16f(w, 0x7410) - 8421376.0f; }
+QCU_D float hi16(int w) { return u16f(w, 0x7432) - 8421376.0f; }
+QCU_D int pack16(float a, float b) {  // |a|, |b| <= 32767.49
+  unsigned ia = __float_as_uint(a + 8421376.0f);
+  unsigned ib = __float_as_uint(b + 8421376.0f);
   return (int)__byte_perm(ia, ib, 0x5410);
 }
 
@@ -272,23 +273,14 @@ template <> struct CloverIO<PREC_DOUBLE> {
   }
 };
 
-// single and half: the 36 reals of block b are reals [36b, 36b+36) of the
-// site's 72, in the order d0..d5, o0.re, o0.im, ..., o14.re, o14.im
+// single: the two blocks interleaved element by element, so that one 16-byte
+// chunk holds the same two elements of both blocks: element e of block b
+// (e = 0..35 in the order d0..d5, o0.re, o0.im, ..., o14.re, o14.im) is float
+// 2e+b of the site's 72, i.e. chunk q = (b0[2q], b1[2q], b0[2q+1], b1[2q+1]).
+// clover_apply_packed multiplies both blocks at once with paired FP32
+// instructions, lane 0 = block 0, lane 1 = block 1.
 template <> struct CloverIO<PREC_SINGLE> {
   typedef float R;
-  static QCU_D void load_block(HermBlock<R>& B, const void* clov, int Vh_pad, int parity, int s, int b) {
-    const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
-    float a[36];
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      float4 w = __ldg(p + chunk_index(b * 9 + k, s, 0, 18, 1));
-      a[4 * k] = w.x; a[4 * k + 1] = w.y; a[4 * k + 2] = w.z; a[4 * k + 3] = w.w;
-    }
-#pragma unroll
-    for (int k = 0; k < 6; k++) B.d[k] = a[k];
-#pragma unroll
-    for (int k = 0; k < 15; k++) B.o[k] = mk(a[6 + 2 * k], a[7 + 2 * k]);
-  }
   template <class RS>
   static QCU_D void store_block(void* clov, int Vh_pad, int parity, int s, int b, const HermBlock<RS>& B, float*) {
     float4* p = static_cast<float4*>(clov) + (size_t)parity * Vh_pad * 18;
@@ -298,7 +290,11 @@ template <> struct CloverIO<PREC_SINGLE> {
 #pragma unroll
     for (int k = 0; k < 15; k++) { a[6 + 2 * k] = (float)B.o[k].re; a[7 + 2 * k] = (float)B.o[k].im; }
 #pragma unroll
-    for (int k = 0; k < 9; k++) p[chunk_index(b * 9 + k, s, 0, 18, 1)] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+    for (int q = 0; q < 18; q++) {
+      float* c = reinterpret_cast<float*>(p + chunk_index(q, s, 0, 18, 1));
+      c[b] = a[2 * q];
+      c[2 + b] = a[2 * q + 1];
+    }
   }
 };
 
@@ -363,11 +359,105 @@ template <> struct CloverIO<PREC_HALF> {
   }
 };
 
+// v <- blockdiag(B0, B1) v with the single-precision clover, both blocks in
+// the two lanes of paired FP32 instructions (sm_100 FFMA2/FMUL2): per site
+// 12 paired multiplies and 120 paired FMAs instead of twice as many scalar ones.
+QCU_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+QCU_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+QCU_D float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+QCU_D float2 fneg2(float2 a) { return make_float2(-a.x, -a.y); }
+QCU_D float2 splat2(float a) { return make_float2(a, a); }
+
+QCU_D void clover_apply_packed(Spinor<float>& v, const void* clov, int Vh_pad, int parity, int s) {
+  const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
+  float2 D[6], Mre[15], Mim[15];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const float4 w = __ldg(p + chunk_index(q, s, 0, 18, 1));
+    D[2 * q] = make_float2(w.x, w.y);
+    D[2 * q + 1] = make_float2(w.z, w.w);
+  }
+#pragma unroll
+  for (int k = 0; k < 15; k++) {
+    const float4 w = __ldg(p + chunk_index(3 + k, s, 0, 18, 1));
+    Mre[k] = make_float2(w.x, w.y);
+    Mim[k] = make_float2(w.z, w.w);
+  }
+  float2 Vre[6], Vim[6], Ore[6], Oim[6];
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    Vre[j] = make_float2(v.c[j].re, v.c[6 + j].re);
+    Vim[j] = make_float2(v.c[j].im, v.c[6 + j].im);
+    Ore[j] = fmul2(D[j], Vre[j]);
+    Oim[j] = fmul2(D[j], Vim[j]);
+  }
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      const int k = tri_index(i, j);
+      // o_i += M_ij v_j
+      Ore[i] = ffma2(Mre[k], Vre[j], Ore[i]);
+      Ore[i] = ffma2(fneg2(Mim[k]), Vim[j], Ore[i]);
+      Oim[i] = ffma2(Mre[k], Vim[j], Oim[i]);
+      Oim[i] = ffma2(Mim[k], Vre[j], Oim[i]);
+      // o_j += conj(M_ij) v_i
+      Ore[j] = ffma2(Mre[k], Vre[i], Ore[j]);
+      Ore[j] = ffma2(Mim[k], Vim[i], Ore[j]);
+      Oim[j] = ffma2(Mre[k], Vim[i], Oim[j]);
+      Oim[j] = ffma2(fneg2(Mim[k]), Vre[i], Oim[j]);
+    }
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    v.c[j] = mk(Ore[j].x, Oim[j].x);
+    v.c[6 + j] = mk(Ore[j].y, Oim[j].y);
+  }
+}
+
 // v <- blockdiag(B0, B1) v with the site's packed clover (one block at a time
-// for double/single; the 16-bit form is fetched in one go, 9 x 16 bytes).
+// for double; the 16-bit form is fetched in one go, 9 x 16 bytes).
+// The same with scalar FP32 instructions, one block after the other.
+QCU_D void clover_apply_single_scalar(Spinor<float>& v, const void* clov, int Vh_pad, int parity, int s) {
+  const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
+  float4 w[18];
+#pragma unroll
+  for (int q = 0; q < 18; q++) w[q] = __ldg(p + chunk_index(q, s, 0, 18, 1));
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    HermBlock<float> B;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      B.d[2 * q] = b ? w[q].y : w[q].x;
+      B.d[2 * q + 1] = b ? w[q].w : w[q].z;
+    }
+#pragma unroll
+    for (int k = 0; k < 15; k++) B.o[k] = b ? mk(w[3 + k].y, w[3 + k].w) : mk(w[3 + k].x, w[3 + k].z);
+    Cplx<float> t[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) t[i] = v.c[6 * b + i];
+    herm_apply(B, t);
+#pragma unroll
+    for (int i = 0; i < 6; i++) v.c[6 * b + i] = t[i];
+  }
+}
+
+// Paired (1) or scalar (0) FP32 clover multiply. Measured on B200 at 32^4 in
+// the fused CG stencil: no gain from pairing (117 vs 120 us at 1 RHS, 1349 vs
+// 1369 us at 16 RHS), so the scalar form is the default.
+#ifndef QCU_CLOVER_FFMA2
+#define QCU_CLOVER_FFMA2 0
+#endif
+
 template <int P, class R>
 QCU_D void clover_apply_site(Spinor<R>& v, const void* clov, int Vh_pad, int parity, int s) {
-  if constexpr (P == PREC_HALF) {
+  if constexpr (P == PREC_SINGLE) {
+    static_assert(sizeof(R) == sizeof(float), "the single-precision clover is applied in FP32");
+#if QCU_CLOVER_FFMA2
+    clover_apply_packed(v, clov, Vh_pad, parity, s);
+#else
+    clover_apply_single_scalar(v, clov, Vh_pad, parity, s);
+#endif
+  } else if constexpr (P == PREC_HALF) {
     const int4* p = static_cast<const int4*>(clov) + (size_t)parity * Vh_pad * 9;
     int4 w[9];
 #pragma unroll

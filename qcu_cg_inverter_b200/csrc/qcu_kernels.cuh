@@ -15,6 +15,9 @@ namespace qcu {
 //   EPI_CPOST          : out = C (x + a h)       (needs EPI_XPAY)
 //   EPI_OUT2           : also out2 = C out
 //   EPI_NORM           : reduce |out|^2 per RHS (finishing functor FinId)
+//   EPI_CGXR           : the CG update instead of a store (needs EPI_XPAY):
+//                        xacc += alpha pvec, racc -= alpha out, reduce
+//                        |racc|^2 (FinCgBeta); out never reaches memory
 enum EpiFlags : int {
   EPI_CPRE = 1,
   EPI_XPAY = 2,
@@ -22,6 +25,7 @@ enum EpiFlags : int {
   EPI_CPOST = 8,
   EPI_OUT2 = 16,
   EPI_NORM = 32,
+  EPI_CGXR = 64,
 };
 
 struct DslashArgs {
@@ -41,6 +45,11 @@ struct DslashArgs {
   double bc_t;
   const int* active;     // per-RHS mask, nullptr -> all active
   ReduceArgs red;
+  // EPI_CGXR: solution and residual in the accumulator precision (double for
+  // FP64 spinors, else single), search direction in the spinor precision
+  SpinorView xacc, racc;
+  CSpinorView pvec;
+  const double* alpha;
 };
 
 // Finishing functors available to fused reductions (see solver kernels).

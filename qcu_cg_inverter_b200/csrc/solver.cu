@@ -16,9 +16,10 @@
 // true residual |b - M x| / |b| in FP64 and the solve stops on it.
 //
 // Inner iterations run in the sloppy precision (16-bit or single storage,
-// FP32 arithmetic; or FP64), six fused kernels per iteration, all scalars
-// on the device. Chunks of iterations are replayed as CUDA graphs; the host
-// looks at the per-RHS state once per chunk.
+// FP32 arithmetic; or FP64), five fused kernels per iteration (four stencils,
+// the last of which also updates x and r, and p = r + beta p), all scalars on
+// the device. Chunks of iterations are replayed as CUDA graphs; the host looks
+// at the per-RHS state once per chunk.
 #include <math.h>
 #include <string.h>
 
@@ -163,7 +164,7 @@ ReduceArgs red_into(const OpCtx& o, double* result, bool with_state) {
   return r;
 }
 
-// One sloppy CG iteration (six launches), masked by the active flags.
+// One sloppy CG iteration (five launches), masked by the active flags.
 int sloppy_iteration(const OpCtx& o) {
   SolverWorkspace& w = *o.w;
   const int ps = w.op;  // operator variant of the sloppy stencils
@@ -188,25 +189,29 @@ int sloppy_iteration(const OpCtx& o) {
     DslashArgs a = op_args(o, ps, 1, w.clover ? w.u : w.y, w.t, act);
     QCU_CHECK(dsl(o, ps, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
   }
-  // z = y - k^2 D^dag_eo t
+  // z = y - k^2 D^dag_eo t, and in the same kernel x += alpha p, r -= alpha z,
+  // rr -> beta (z stays in registers)
   {
     DslashArgs a = op_args(o, ps, 0, w.t, w.z, act);
     a.x = w.y.cview(0);
     a.coef = w.dd(D_MK2);
-    QCU_CHECK(dsl(o, ps, true, EPI_XPAY, FIN_NONE, a));
+    a.xacc = w.xlo.view(0);
+    a.racc = w.rlo.view(0);
+    a.pvec = w.p.cview(0);
+    a.alpha = w.st.alpha;
+    a.red = red_into(o, o.ctx->red.result.as<double>(), true);
+    QCU_CHECK(dsl(o, ps, true, EPI_XPAY | EPI_CGXR, FIN_CG_BETA, a));
   }
-  // x += alpha p, r -= alpha z, rr -> beta
-  QCU_CHECK_CUDA(launch_cg_xr(w.pa, w.ps, o.ctx->g.Vh, w.nrhs, w.xlo.view(0), w.rlo.view(0), w.p.cview(0), w.z.cview(0),
-                              w.st.alpha, act, red_into(o, o.ctx->red.result.as<double>(), true), w.shape, o.st));
   // p = r + beta p
   QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, o.ctx->g.Vh, w.nrhs, w.p.view(0), w.rlo.cview(0), w.st.beta, act, w.shape, o.st));
-  o.ctx->launches += 2;
+  o.ctx->launches += 1;
   return QCU_SUCCESS;
 }
 
-// FP64 true residual for the RHS in mask `upd`: x_hi += x_lo, r = bhat - Mhat
-// x_hi, |r|^2, |A_ee r|^2 (the full-system residual), r_ne = Mhat^dag r and
-// |r_ne|^2 (into D_RES_R2, D_RES_AR2, D_RES_NE).
+// True residual for the RHS in mask `upd`: x_hi += x_lo, then in FP64
+// r = bhat - Mhat x_hi, |r|^2 and |A_ee r|^2 (the full-system residual), and
+// r_ne = Mhat^dag r with |r_ne|^2 (into D_RES_R2, D_RES_AR2, D_RES_NE; r_ne
+// lands in z, of the sloppy precision, or z64 for FP64 inner solves).
 int reliable_update(const OpCtx& o) {
   SolverWorkspace& w = *o.w;
   const int* upd = w.di(I_UPD);
@@ -238,16 +243,35 @@ int reliable_update(const OpCtx& o) {
                                        w.di(I_CIDX), upd, nullptr, w.shape, o.st));
     o.ctx->launches += 2;
   }
-  {
-    DslashArgs a = op_args(o, PREC_DOUBLE, 1, w.clover ? w.u64 : w.y64, w.t64, upd);
-    QCU_CHECK(dsl(o, PREC_DOUBLE, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  // r_ne = Mhat^dag r only restarts the sloppy recursion (convergence is
+  // decided on the FP64 |A_ee r| above), so with sloppy inner precision it is
+  // computed by the sloppy operator from r (and A_ee^-1 r) rounded to the
+  // sloppy storage; with FP64 inner precision it stays in FP64
+  const bool sloppy_ne = w.ps != PREC_DOUBLE;
+  const int pn = sloppy_ne ? w.op : PREC_DOUBLE;
+  const Field& rin = sloppy_ne ? w.y : w.y64;
+  const Field& uin = sloppy_ne ? w.u : w.u64;
+  const Field& tn = sloppy_ne ? w.t : w.t64;
+  const Field& zn = sloppy_ne ? w.z : w.z64;
+  if (sloppy_ne) {
+    QCU_CHECK_CUDA(launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.y.view(0), w.y64.cview(0), upd, nullptr, w.shape, o.st));
+    o.ctx->launches++;
+    if (w.clover) {
+      QCU_CHECK_CUDA(
+          launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.u.view(0), w.u64.cview(0), upd, nullptr, w.shape, o.st));
+      o.ctx->launches++;
+    }
   }
   {
-    DslashArgs a = op_args(o, PREC_DOUBLE, 0, w.t64, w.z64, upd);
-    a.x = w.y64.cview(0);
+    DslashArgs a = op_args(o, pn, 1, w.clover ? uin : rin, tn, upd);
+    QCU_CHECK(dsl(o, pn, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
+  }
+  {
+    DslashArgs a = op_args(o, pn, 0, tn, zn, upd);
+    a.x = rin.cview(0);
     a.coef = w.dd(D_MK2);
     a.red = red_into(o, w.dd(D_RES_NE), false);
-    QCU_CHECK(dsl(o, PREC_DOUBLE, true, EPI_XPAY | EPI_NORM, FIN_NONE, a));
+    QCU_CHECK(dsl(o, pn, true, EPI_XPAY | EPI_NORM, FIN_NONE, a));
   }
   return QCU_SUCCESS;
 }
@@ -296,8 +320,9 @@ int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select) {
   rel_decide_kernel<<<nb, tb, 0, o.st>>>(nrhs, w.mem.as<double>(), w.di(0), P);
   QCU_CHECK_CUDA(cudaGetLastError());
   const int Vh = o.ctx->g.Vh;
-  QCU_CHECK_CUDA(launch_convert(w.pa, PREC_DOUBLE, Vh, nrhs, w.rlo.view(0), w.z64.cview(0), w.di(I_RST), nullptr,
-                                w.shape, o.st));
+  const bool sloppy_ne = w.ps != PREC_DOUBLE;  // where reliable_update left r_ne
+  QCU_CHECK_CUDA(launch_convert(w.pa, sloppy_ne ? w.ps : PREC_DOUBLE, Vh, nrhs, w.rlo.view(0),
+                                sloppy_ne ? w.z.cview(0) : w.z64.cview(0), w.di(I_RST), nullptr, w.shape, o.st));
   QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, Vh, nrhs, w.p.view(0), w.rlo.cview(0), w.dd(D_BETA), w.di(I_RST), w.shape, o.st));
   o.ctx->launches += 3;
   return QCU_SUCCESS;
