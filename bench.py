@@ -425,9 +425,12 @@ def run_multi(args):
     t64, it64 = [], []
     for j, k in enumerate(MULTI_KAPPAS):
         bb = b[12 * j].contiguous()
-        t, r = timed(lambda: ctx.invert(x1, bb, kappa=k, precision="double", **kw)[0])
-        assert r["converged"], r
-        t64.append(t)
+        ts = []
+        for _ in range(2):  # two timings per kappa, the faster one kept
+            t, r = timed(lambda: ctx.invert(x1, bb, kappa=k, precision="double", **kw)[0])
+            assert r["converged"], r
+            ts.append(t)
+        t64.append(min(ts))
         it64.append(r["iterations"])
     per64 = sum(t64) / len(t64)
     ctx.close()

@@ -28,8 +28,21 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_MINB16_OUT2
 #define QCU_DSLASH_MINB16_OUT2 3
 #endif
+// likewise the hop + A^-1 kernel (measured in the 48-RHS 24^3x48 solve:
+// 0.600 vs 0.605 s); the kernel with the fused CG update stays at 128
+// registers (0.660 s with the 85-register cap)
+#ifndef QCU_DSLASH_MINB16_CPRE
+#define QCU_DSLASH_MINB16_CPRE 3
+#endif
+#ifndef QCU_DSLASH_MINB16_CGXR
+#define QCU_DSLASH_MINB16_CGXR 2
+#endif
 constexpr int dslash_minb(int op, int epi) {
-  return (op_spinor_prec(op) == PREC_HALF && (epi & EPI_OUT2)) ? QCU_DSLASH_MINB16_OUT2 : QCU_DSLASH_MINB;
+  return op_spinor_prec(op) != PREC_HALF ? QCU_DSLASH_MINB
+         : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
+         : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
+         : (epi == EPI_CPRE)             ? QCU_DSLASH_MINB16_CPRE
+                                         : QCU_DSLASH_MINB;
 }
 
 // OP selects the storage of spinors, links and clover (OpVariant).
