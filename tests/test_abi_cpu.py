@@ -77,3 +77,16 @@ def test_bad_lattice_rejected(qcu_lib):
     h = ctypes.c_void_p()
     L4 = (ctypes.c_int * 4)(7, 8, 8, 8)  # odd Lx
     assert qcu_lib.lib().qcuContextCreate(ctypes.byref(h), L4, 0) == qcu_lib.QCU_ERR_INVALID_ARG
+
+
+def test_server_param_defaults(qcu_lib):
+    sp = qcu_lib.server_params()
+    assert sp.precision == qcu_lib.PREC_HALF and sp.tol == 1e-10 and sp.maxiter == 20000 and sp.bc_t == -1.0
+    assert sp.columns == 16 and sp.clover_slots == 8 and sp.device_budget == 0 and sp.autotune == 1
+
+
+def test_server_entry_points_are_declared(qcu_lib):
+    names = declared_functions()
+    for n in ("qcuServerCreate", "qcuServerSubmit", "qcuServerPoll", "qcuServerQuery", "qcuServerRunTrace",
+              "qcuServerDestroy", "qcuHostAlloc"):
+        assert n in names
