@@ -122,6 +122,31 @@ __global__ void __launch_bounds__(256) accumulate_kernel(int nsites, int nrhs, S
   SpinorIO<PL>::store(xlo, s, r, l);
 }
 
+// xhi += xlo ; xlo = 0 ; d = b - xhi (the start of r = bhat - Mhat xhi, which
+// the next stencil completes as d + kappa^2 A^-1 D t)
+template <int PL>
+__global__ void __launch_bounds__(256) accumulate_res_kernel(int nsites, int nrhs, SpinorView xhi, SpinorView xlo,
+                                                             CSpinorView b, SpinorView d, const int* active) {
+  typedef typename CompReal<PL>::type RL;
+  QCU_SITE_RHS
+  if (!valid) return;
+  Spinor<double> h, bv;
+  Spinor<RL> l;
+  SpinorIO<PREC_DOUBLE>::load(h, xhi, s, r);
+  SpinorIO<PL>::load(l, xlo, s, r);
+  SpinorIO<PREC_DOUBLE>::load(bv, b, s, r);
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    h.c[k].re += (double)l.c[k].re;
+    h.c[k].im += (double)l.c[k].im;
+    l.c[k] = mk(RL(0), RL(0));
+    bv.c[k] = bv.c[k] - h.c[k];
+  }
+  SpinorIO<PREC_DOUBLE>::store(xhi, s, r, h);
+  SpinorIO<PL>::store(xlo, s, r, l);
+  SpinorIO<PREC_DOUBLE>::store(d, s, r, bv);
+}
+
 // f = 0 on the RHS in the mask (16-bit fields: norm 0 too)
 template <int P>
 __global__ void __launch_bounds__(256) zero_kernel(int nsites, int nrhs, SpinorView f, const int* active) {
@@ -285,6 +310,15 @@ cudaError_t launch_zero(int prec, int nsites, int nrhs, SpinorView f, const int*
     case PREC_HALF: zero_kernel<PREC_HALF><<<g, b, 0, st>>>(nsites, nrhs, f, active); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate_res(int pl, int nsites, int nrhs, SpinorView xhi, SpinorView xlo, CSpinorView b,
+                                  SpinorView d, const int* active, LaunchShape sh, cudaStream_t st) {
+  dim3 bl = blk(sh), g = grd(nsites, nrhs, sh);
+  if (pl == PREC_DOUBLE) accumulate_res_kernel<PREC_DOUBLE><<<g, bl, 0, st>>>(nsites, nrhs, xhi, xlo, b, d, active);
+  else if (pl == PREC_SINGLE) accumulate_res_kernel<PREC_SINGLE><<<g, bl, 0, st>>>(nsites, nrhs, xhi, xlo, b, d, active);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

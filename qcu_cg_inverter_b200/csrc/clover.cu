@@ -322,6 +322,39 @@ __global__ void __launch_bounds__(256) clover_apply_kernel(Geom g, int parity, i
   }
 }
 
+// |A r|^2 (reduced per RHS) and u = A^-1 r, FP64, one read of r
+__global__ void __launch_bounds__(256) clover_res_kernel(Geom g, int parity, int nrhs, CSpinorView rin, SpinorView u,
+                                                         const void* A, const void* Ainv, size_t clov_stride,
+                                                         const int* clov_idx, const int* active, ReduceArgs red) {
+  const int r = blockIdx.y * blockDim.x + threadIdx.x;
+  const int s = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool valid = (s < g.Vh) && (r < nrhs) && (active == nullptr || active[r]);
+  double nrm = 0.0;
+  if (valid) {
+    Spinor<double> v, w;
+    SpinorIO<PREC_DOUBLE>::load(v, rin, s, r);
+    w = v;
+    const int ci = clov_idx ? clov_idx[r] : 0;
+    if (ci >= 0) {  // negative slot: A = 1
+      clover_apply_site<PREC_DOUBLE>(v, static_cast<const char*>(A) + clov_stride * (size_t)ci, g.Vh_pad, parity, s);
+      clover_apply_site<PREC_DOUBLE>(w, static_cast<const char*>(Ainv) + clov_stride * (size_t)ci, g.Vh_pad, parity, s);
+    }
+    SpinorIO<PREC_DOUBLE>::store(u, s, r, w);
+    for (int k = 0; k < 12; k++) nrm += v.c[k].re * v.c[k].re + v.c[k].im * v.c[k].im;
+  }
+  double vv[1] = {nrm};
+  block_reduce_finish<1, FinNone>(vv, nrhs, red);
+}
+
+cudaError_t launch_clover_res(const Geom& g, int parity, int nrhs, CSpinorView r, SpinorView u, const void* A,
+                              const void* Ainv, size_t clov_stride, const int* clov_idx, const int* active,
+                              const ReduceArgs& red, LaunchShape sh, cudaStream_t stream) {
+  dim3 block(sh.Rb, sh.Sb);
+  dim3 grid(grid_x(g.Vh, sh.Sb), (nrhs + sh.Rb - 1) / sh.Rb);
+  clover_res_kernel<<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, A, Ainv, clov_stride, clov_idx, active, red);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_clover_apply(int prec, const Geom& g, int parity, int nrhs, CSpinorView in, SpinorView out,
                                 const void* clov, size_t clov_stride, const int* clov_idx, const int* active,
                                 const ReduceArgs* red, LaunchShape sh, cudaStream_t stream) {

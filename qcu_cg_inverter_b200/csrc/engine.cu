@@ -29,6 +29,7 @@ __global__ void slot_init_kernel(int nrhs, double* dmem, int* imem, int r0, int 
   dmem[(size_t)D_RROLD * nrhs + r] = __longlong_as_double(0x7ff0000000000000LL);  // +inf: beta = 0 at the first update
   dmem[(size_t)D_KAPPA * nrhs + r] = kappa;
   dmem[(size_t)D_MK2 * nrhs + r] = -kappa * kappa;
+  dmem[(size_t)D_K2 * nrhs + r] = kappa * kappa;
   imem[(size_t)I_CIDX * nrhs + r] = cidx;
   if (admit) {
     imem[(size_t)I_EVENT * nrhs + r] = 1;

@@ -76,6 +76,24 @@ QCU_D int pack16(float a, float b) {  // |a|, |b| <= 32767.49
   return (int)__byte_perm(ia, ib, 0x5410);
 }
 
+// Paired FP32 instructions of sm_100 (FFMA2 / FMUL2 / FADD2): two lanes per
+// instruction, each lane rounded exactly as the scalar instruction.
+QCU_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+QCU_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+QCU_D float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+QCU_D float2 fneg2(float2 a) { return make_float2(-a.x, -a.y); }
+QCU_D float2 splat2(float a) { return make_float2(a, a); }
+
+// (re, im) of one 16-bit word, scaled: the same roundings as lo16/hi16 times nm
+QCU_D float2 dec16_pair(int w, float nm) {
+  return fmul2(fadd2(make_float2(u16f(w, 0x7410), u16f(w, 0x7432)), splat2(-8421376.0f)), splat2(nm));
+}
+// one 16-bit word from (re, im) times sc: the same roundings as pack16(re*sc, im*sc)
+QCU_D int enc16_pair(float re, float im, float sc) {
+  const float2 t = fadd2(fmul2(make_float2(re, im), splat2(sc)), splat2(8421376.0f));
+  return (int)__byte_perm(__float_as_uint(t.x), __float_as_uint(t.y), 0x5410);
+}
+
 template <> struct SpinorIO<PREC_HALF> {
   typedef float R;
   // integer-valued components (not yet scaled) and the factor that scales them
@@ -97,10 +115,12 @@ template <> struct SpinorIO<PREC_HALF> {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       int4 w = p[chunk_index(c, s, r, 3, f.nrhs)];
-      v.c[4 * c + 0] = mk(lo16(w.x) * nm, hi16(w.x) * nm);
-      v.c[4 * c + 1] = mk(lo16(w.y) * nm, hi16(w.y) * nm);
-      v.c[4 * c + 2] = mk(lo16(w.z) * nm, hi16(w.z) * nm);
-      v.c[4 * c + 3] = mk(lo16(w.w) * nm, hi16(w.w) * nm);
+      const int ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const float2 q = dec16_pair(ws[k], nm);
+        v.c[4 * c + k] = mk(q.x, q.y);
+      }
     }
   }
   static QCU_D void store(const SpinorView& f, int s, int r, const Spinor<R>& v) {
@@ -112,10 +132,10 @@ template <> struct SpinorIO<PREC_HALF> {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       int4 w;
-      w.x = pack16(v.c[4 * c + 0].re * sc, v.c[4 * c + 0].im * sc);
-      w.y = pack16(v.c[4 * c + 1].re * sc, v.c[4 * c + 1].im * sc);
-      w.z = pack16(v.c[4 * c + 2].re * sc, v.c[4 * c + 2].im * sc);
-      w.w = pack16(v.c[4 * c + 3].re * sc, v.c[4 * c + 3].im * sc);
+      w.x = enc16_pair(v.c[4 * c + 0].re, v.c[4 * c + 0].im, sc);
+      w.y = enc16_pair(v.c[4 * c + 1].re, v.c[4 * c + 1].im, sc);
+      w.z = enc16_pair(v.c[4 * c + 2].re, v.c[4 * c + 2].im, sc);
+      w.w = enc16_pair(v.c[4 * c + 3].re, v.c[4 * c + 3].im, sc);
       p[chunk_index(c, s, r, 3, f.nrhs)] = w;
     }
     f.norm[(size_t)s * f.nrhs + r] = mx;
@@ -362,12 +382,6 @@ template <> struct CloverIO<PREC_HALF> {
 // v <- blockdiag(B0, B1) v with the single-precision clover, both blocks in
 // the two lanes of paired FP32 instructions (sm_100 FFMA2/FMUL2): per site
 // 12 paired multiplies and 120 paired FMAs instead of twice as many scalar ones.
-QCU_D float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-QCU_D float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-QCU_D float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-QCU_D float2 fneg2(float2 a) { return make_float2(-a.x, -a.y); }
-QCU_D float2 splat2(float a) { return make_float2(a, a); }
-
 QCU_D void clover_apply_packed(Spinor<float>& v, const void* clov, int Vh_pad, int parity, int s) {
   const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
   float2 D[6], Mre[15], Mim[15];

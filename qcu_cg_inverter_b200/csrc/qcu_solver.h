@@ -15,8 +15,8 @@ namespace qcu {
 // each nrhs long (SolverWorkspace::mem); the host mirror has the same layout.
 // D_RRPRE: the iterated |r|^2 just before the last reliable update (the end
 // point of the convergence segment it closed).
-enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_RES_R2, D_RES_AR2, D_RES_NE, D_BNORM,
-       D_TRUE, D_RRPRE, D_NUM };
+enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_K2, D_RES_R2, D_RES_AR2, D_RES_NE,
+       D_BNORM, D_TRUE, D_RRPRE, D_NUM };  // D_MK2 = -kappa^2, D_K2 = +kappa^2
 // I_ADM: RHS being admitted (source staged, bhat and x = 0 to be set up);
 // I_RET: RHS being retired (solution reconstructed and copied out).
 enum { I_ACTIVE = 0, I_EVENT, I_ITERS, I_BREAK, I_CIDX, I_UPD, I_RST, I_DONE, I_CONV, I_STATUS, I_NUPD, I_ADM, I_RET,

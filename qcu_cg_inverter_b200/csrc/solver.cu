@@ -216,7 +216,10 @@ int reliable_update(const OpCtx& o) {
   SolverWorkspace& w = *o.w;
   const int* upd = w.di(I_UPD);
   const int Vh = o.ctx->g.Vh;
-  QCU_CHECK_CUDA(launch_accumulate(w.pa, Vh, w.nrhs, w.xhi.view(0), w.xlo.view(0), upd, w.shape, o.st));
+  // x_hi += x_lo and y64 = bhat - x_hi, then r = y64 + kappa^2 A_ee^-1 D_eo
+  // A_oo^-1 D_oe x_hi = bhat - Mhat x_hi in place in y64, with |r|^2
+  QCU_CHECK_CUDA(launch_accumulate_res(w.pa, Vh, w.nrhs, w.xhi.view(0), w.xlo.view(0), w.bh.cview(0), w.y64.view(0),
+                                       upd, w.shape, o.st));
   o.ctx->launches++;
   {
     DslashArgs a = op_args(o, PREC_DOUBLE, 1, w.xhi, w.t64, upd);
@@ -224,24 +227,18 @@ int reliable_update(const OpCtx& o) {
   }
   {
     DslashArgs a = op_args(o, PREC_DOUBLE, 0, w.t64, w.y64, upd);
-    a.x = w.xhi.cview(0);
-    a.coef = w.dd(D_MK2);
-    QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? (EPI_CPRE | EPI_XPAY) : EPI_XPAY, FIN_NONE, a));
+    a.x = w.y64.cview(0);  // read and overwritten by the same thread, site by site
+    a.coef = w.dd(D_K2);
+    a.red = red_into(o, w.dd(D_RES_R2), false);
+    QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? (EPI_CPRE | EPI_XPAY | EPI_NORM) : (EPI_XPAY | EPI_NORM), FIN_NONE,
+                  a));
   }
-  // r = bhat - Mhat x (in y64)
-  QCU_CHECK_CUDA(launch_residual(Vh, w.nrhs, w.y64.view(0), w.bh.cview(0), w.y64.cview(0), upd,
-                                 red_into(o, w.dd(D_RES_R2), false), w.shape, o.st));
-  o.ctx->launches++;
-  if (w.clover) {
-    ReduceArgs ra = red_into(o, w.dd(D_RES_AR2), false);
-    SpinorView none{nullptr, nullptr, w.nrhs};
-    QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0), none,
-                                       ctx_clover_ptr(o.ctx, PREC_DOUBLE, false), ctx_clover_stride(o.ctx, PREC_DOUBLE),
-                                       w.di(I_CIDX), upd, &ra, w.shape, o.st));
-    QCU_CHECK_CUDA(launch_clover_apply(PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0), w.u64.view(0),
-                                       ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
-                                       w.di(I_CIDX), upd, nullptr, w.shape, o.st));
-    o.ctx->launches += 2;
+  if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass
+    QCU_CHECK_CUDA(launch_clover_res(o.ctx->g, 0, w.nrhs, w.y64.cview(0), w.u64.view(0),
+                                     ctx_clover_ptr(o.ctx, PREC_DOUBLE, false), ctx_clover_ptr(o.ctx, PREC_DOUBLE, true),
+                                     ctx_clover_stride(o.ctx, PREC_DOUBLE), w.di(I_CIDX), upd,
+                                     red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
+    o.ctx->launches++;
   }
   // r_ne = Mhat^dag r only restarts the sloppy recursion (convergence is
   // decided on the FP64 |A_ee r| above), so with sloppy inner precision it is
