@@ -179,8 +179,8 @@ int make_resident(qcu_server_s* s, int id) {
     return st;
   }
   R.ctx = ctx;
+  R.bytes = qcuContextDeviceBytes(ctx) + eng->device_bytes();  // the engine is not the context's own
   R.eng = std::move(eng);
-  R.bytes = qcuContextDeviceBytes(ctx);
   R.last_use = ++s->clock;
   return QCU_SUCCESS;
 }
