@@ -9,6 +9,7 @@ DslashKernelFn pick_f64(bool dag, int epi, int fin);
 DslashKernelFn pick_f32(bool dag, int epi, int fin);
 DslashKernelFn pick_f16(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x(bool dag, int epi, int fin);
+DslashKernelFn pick_f16x1(bool dag, int epi, int fin);
 
 cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape sh,
                           cudaStream_t stream) {
@@ -17,7 +18,7 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
     case PREC_DOUBLE: fn = pick_f64(dagger, epi, fin); break;
     case PREC_SINGLE: fn = pick_f32(dagger, epi, fin); break;
     case PREC_HALF: fn = pick_f16(dagger, epi, fin); break;
-    case OP_HALF_FAST: fn = pick_f16x(dagger, epi, fin); break;
+    case OP_HALF_FAST: fn = a.nrhs == 1 ? pick_f16x1(dagger, epi, fin) : pick_f16x(dagger, epi, fin); break;
     default: break;
   }
   if (!fn) return cudaErrorInvalidValue;

@@ -185,10 +185,14 @@ enum OpVariant : int {
   OP_SINGLE = 1,     // FP32 spinors, FP32 12-real links, FP32 clover
   OP_HALF = 2,       // 16-bit spinors, 16-bit 12-real links, 16-bit clover
   OP_HALF_FAST = 3,  // 16-bit spinors, FP32 18-real links, FP32 clover
+  // the same storage as OP_HALF_FAST; the kernels its launches use for a
+  // single RHS (block-paired epilogues at 128 registers)
+  OP_HALF_FAST_1 = 4,
 };
-__host__ __device__ constexpr int op_spinor_prec(int op) { return op == OP_HALF_FAST ? (int)PREC_HALF : op; }
-__host__ __device__ constexpr int op_link_format(int op) { return op == OP_HALF_FAST ? (int)LINK_SINGLE18 : op; }
-__host__ __device__ constexpr int op_clover_prec(int op) { return op == OP_HALF_FAST ? (int)PREC_SINGLE : op; }
+__host__ __device__ constexpr bool op_fast(int op) { return op == OP_HALF_FAST || op == OP_HALF_FAST_1; }
+__host__ __device__ constexpr int op_spinor_prec(int op) { return op_fast(op) ? (int)PREC_HALF : op; }
+__host__ __device__ constexpr int op_link_format(int op) { return op_fast(op) ? (int)LINK_SINGLE18 : op; }
+__host__ __device__ constexpr int op_clover_prec(int op) { return op_fast(op) ? (int)PREC_SINGLE : op; }
 
 // 16-bit storage is fixed point: a real v in [-1,1] is stored as
 // round(v*32767); spinors and clover blocks carry one float norm per site so

@@ -281,10 +281,9 @@ QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, 
 }
 
 template <int PL, bool DAG>
-QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, int r, const CSpinorView& in,
+QCU_D void hop_spin_pair(SpinPair& o, const Geom& g, int parity, int s, int r, const CSpinorView& in,
                          const void* gauge, float bc_t) {
   constexpr int F = DAG ? -1 : 1;
-  SpinPair o;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     o.ure[c] = o.uim[c] = o.lre[c] = o.lim[c] = o.xre[c] = o.xim[c] = make_float2(0.f, 0.f);
@@ -294,6 +293,13 @@ QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, i
   hop_dir_pair<PL, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
   hop_dir_pair<PL, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
   hop_dir_pair<PL, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+}
+
+template <int PL, bool DAG>
+QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, int r, const CSpinorView& in,
+                         const void* gauge, float bc_t) {
+  SpinPair o;
+  hop_spin_pair<PL, DAG>(o, g, parity, s, r, in, gauge, bc_t);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     out.c[c] = mk(o.ure[c].x, o.uim[c].x);
@@ -301,6 +307,123 @@ QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, i
     out.c[6 + c] = mk(o.lre[c].x + o.xre[c].y, o.lim[c].x + o.xim[c].y);
     out.c[9 + c] = mk(o.lre[c].y + o.xre[c].x, o.lim[c].y + o.xim[c].x);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Block-paired spinors for the fast 16-bit operator's epilogues: pair j holds
+// component j of chiral block 0 (spins 0,1) in lane 0 and component j of
+// block 1 (spins 2,3) in lane 1, i.e. (c[j], c[6+j]). The two 6x6 clover
+// blocks then multiply both halves of the spinor in one paired instruction
+// each, with the block-interleaved FP32 clover supplying matching pairs, and
+// xpay, the 16-bit decode and encode and the norm stay paired too.
+// ---------------------------------------------------------------------------
+struct SpinBlock {
+  float2 re[6], im[6];
+};
+
+template <int PL, bool DAG>
+QCU_D void hop_half_block(SpinBlock& out, const Geom& g, int parity, int s, int r, const CSpinorView& in,
+                          const void* gauge, float bc_t) {
+  SpinPair o;
+  hop_spin_pair<PL, DAG>(o, g, parity, s, r, in, gauge, bc_t);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {  // spin 0 and 2 of colour c, then spin 1 and 3
+    out.re[c] = make_float2(o.ure[c].x, o.lre[c].x + o.xre[c].y);
+    out.im[c] = make_float2(o.uim[c].x, o.lim[c].x + o.xim[c].y);
+    out.re[3 + c] = make_float2(o.ure[c].y, o.lre[c].y + o.xre[c].x);
+    out.im[3 + c] = make_float2(o.uim[c].y, o.lim[c].y + o.xim[c].x);
+  }
+}
+
+// v <- blockdiag(B0, B1) v, FP32 block-interleaved clover
+QCU_D void clover_apply_block(SpinBlock& v, const void* clov, int Vh_pad, int parity, int s) {
+  const float4* p = static_cast<const float4*>(clov) + (size_t)parity * Vh_pad * 18;
+  float2 ore[6], oim[6];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const float4 w = __ldg(p + chunk_index(q, s, 0, 18, 1));
+    const float2 d0 = make_float2(w.x, w.y), d1 = make_float2(w.z, w.w);
+    ore[2 * q] = fmul2(d0, v.re[2 * q]);
+    oim[2 * q] = fmul2(d0, v.im[2 * q]);
+    ore[2 * q + 1] = fmul2(d1, v.re[2 * q + 1]);
+    oim[2 * q + 1] = fmul2(d1, v.im[2 * q + 1]);
+  }
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      const float4 w = __ldg(p + chunk_index(3 + tri_index(i, j), s, 0, 18, 1));
+      const float2 mre = make_float2(w.x, w.y), mim = make_float2(w.z, w.w);
+      // o_i += M_ij v_j ; o_j += conj(M_ij) v_i
+      ore[i] = ffma2(mre, v.re[j], ore[i]);
+      ore[i] = ffma2(fneg2(mim), v.im[j], ore[i]);
+      oim[i] = ffma2(mre, v.im[j], oim[i]);
+      oim[i] = ffma2(mim, v.re[j], oim[i]);
+      ore[j] = ffma2(mre, v.re[i], ore[j]);
+      ore[j] = ffma2(mim, v.im[i], ore[j]);
+      oim[j] = ffma2(mre, v.im[i], oim[j]);
+      oim[j] = ffma2(fneg2(mim), v.re[i], oim[j]);
+    }
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    v.re[j] = ore[j];
+    v.im[j] = oim[j];
+  }
+}
+
+QCU_D void load16_block(SpinBlock& v, const CSpinorView& f, int s, int r) {
+  const int4* p = static_cast<const int4*>(f.data);
+  int4 w[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) w[c] = p[chunk_index(c, s, r, 3, f.nrhs)];
+  const float2 nm = splat2(f.norm[(size_t)s * f.nrhs + r] * kInvFix);
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    const int a = word_of(w, j), b = word_of(w, 6 + j);
+    v.re[j] = fmul2(dec_lo2(a, b), nm);
+    v.im[j] = fmul2(dec_hi2(a, b), nm);
+  }
+}
+
+QCU_D void store16_block(const SpinorView& f, int s, int r, const SpinBlock& v) {
+  float mx = 0.f;
+#pragma unroll
+  for (int j = 0; j < 6; j++)
+    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.re[j].x), fabsf(v.re[j].y)), fmaxf(fabsf(v.im[j].x), fabsf(v.im[j].y))));
+  const float sc = mx > 0.f ? kFix / mx : 0.f;
+  float2 tre[6], tim[6];
+#pragma unroll
+  for (int j = 0; j < 6; j++) {  // the roundings of pack16(x * sc, ...)
+    tre[j] = fadd2(fmul2(v.re[j], splat2(sc)), splat2(8421376.0f));
+    tim[j] = fadd2(fmul2(v.im[j], splat2(sc)), splat2(8421376.0f));
+  }
+  int words[12];
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    words[j] = (int)__byte_perm(__float_as_uint(tre[j].x), __float_as_uint(tim[j].x), 0x5410);
+    words[6 + j] = (int)__byte_perm(__float_as_uint(tre[j].y), __float_as_uint(tim[j].y), 0x5410);
+  }
+  int4* p = static_cast<int4*>(f.data);
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    p[chunk_index(c, s, r, 3, f.nrhs)] = make_int4(words[4 * c], words[4 * c + 1], words[4 * c + 2], words[4 * c + 3]);
+  f.norm[(size_t)s * f.nrhs + r] = mx;
+}
+
+// |v|^2, summed in FP32 pairs (the sloppy solver's dot products)
+QCU_D float norm2_block(const SpinBlock& v) {
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    acc = ffma2(v.re[j], v.re[j], acc);
+    acc = ffma2(v.im[j], v.im[j], acc);
+  }
+  return acc.x + acc.y;
+}
+
+// component k (= spin*3 + colour) of a block-paired spinor
+QCU_D Cplx<float> block_comp(const SpinBlock& v, int k) {
+  return k < 6 ? mk(v.re[k].x, v.im[k].x) : mk(v.re[k - 6].y, v.im[k - 6].y);
 }
 
 template <int PS, int PL, bool DAG, class R>

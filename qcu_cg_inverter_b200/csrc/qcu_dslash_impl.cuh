@@ -38,11 +38,76 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #define QCU_DSLASH_MINB16_CGXR 2
 #endif
 constexpr int dslash_minb(int op, int epi) {
-  return op_spinor_prec(op) != PREC_HALF ? QCU_DSLASH_MINB
+  return (op_spinor_prec(op) != PREC_HALF || op == OP_HALF_FAST_1) ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
          : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
          : (epi == EPI_CPRE)             ? QCU_DSLASH_MINB16_CPRE
                                          : QCU_DSLASH_MINB;
+}
+
+// Clover field of RHS r: its slot in the bank, or nullptr for a negative slot
+// index (no clover term for that RHS, A = 1), so Wilson and clover systems can
+// share a batch.
+QCU_D const void* clover_of(const DslashArgs& a, int r) {
+  if (!a.clover_idx) return a.clover;
+  const int ci = a.clover_idx[r];
+  return ci >= 0 ? static_cast<const char*>(a.clover) + a.clover_stride * (size_t)ci : nullptr;
+}
+
+// One output site and RHS of the fast 16-bit operator (16-bit spinors, FP32
+// 18-real links, FP32 block-interleaved clover): the hop and every epilogue in
+// block-paired FP32 instructions. Same arithmetic per component as the
+// generic body below; the norms are summed in FP32 before the FP64 block sums.
+template <bool DAG, int EPI>
+QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
+  SpinBlock o;
+  hop_half_block<LINK_SINGLE18, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (float)a.bc_t);
+  const void* clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) ? clover_of(a, r) : nullptr;
+  if (EPI & EPI_CPRE)
+    if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+  if (EPI & EPI_XPAY) {
+    const float2 c = splat2(a.coef ? (float)a.coef[r] : (float)a.coef0);
+    SpinBlock xv;
+    load16_block(xv, a.x, s, r);
+    if (EPI & EPI_CX)
+      if (clov) clover_apply_block(xv, clov, a.g.Vh_pad, a.parity, s);
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      o.re[j] = ffma2(c, o.re[j], xv.re[j]);
+      o.im[j] = ffma2(c, o.im[j], xv.im[j]);
+    }
+    if (EPI & EPI_CPOST)
+      if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+  }
+  if constexpr ((EPI & EPI_CGXR) != 0) {
+    // x += alpha p, r -= alpha out (the out of this kernel is the CG's z)
+    const float al = (float)a.alpha[r];
+    Spinor<float> xv, rv, pv;
+    SpinorIO<PREC_SINGLE>::load(xv, a.xacc, s, r);
+    SpinorIO<PREC_SINGLE>::load(rv, a.racc, s, r);
+    SpinorIO<PREC_HALF>::load(pv, a.pvec, s, r);
+    float n = 0.f;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      const Cplx<float> z = block_comp(o, k);
+      xv.c[k].re += al * pv.c[k].re;
+      xv.c[k].im += al * pv.c[k].im;
+      rv.c[k].re -= al * z.re;
+      rv.c[k].im -= al * z.im;
+      n = fmaf(rv.c[k].re, rv.c[k].re, n);
+      n = fmaf(rv.c[k].im, rv.c[k].im, n);
+    }
+    SpinorIO<PREC_SINGLE>::store(a.xacc, s, r, xv);
+    SpinorIO<PREC_SINGLE>::store(a.racc, s, r, rv);
+    nrm = n;
+  } else {
+    store16_block(a.out, s, r, o);
+    if (EPI & EPI_NORM) nrm = norm2_block(o);
+  }
+  if (EPI & EPI_OUT2) {
+    if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+    store16_block(a.out2, s, r, o);
+  }
 }
 
 // OP selects the storage of spinors, links and clover (OpVariant).
@@ -54,18 +119,15 @@ __global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
   const bool valid = (s < a.g.Vh) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
   double nrm = 0.0;
-  if (valid) {
+  // single-RHS launches of the fast 16-bit operator: block-paired epilogues
+  // (measured: 16^3x32 solve 3.70 vs 3.88 ms); with many RHS per launch the
+  // generic body at the 85-register cap is faster (48-RHS batch 0.592 vs 0.606 s)
+  if (OP == OP_HALF_FAST_1 && valid) {
+    site_half_fast<DAG, EPI>(a, s, r, nrm);
+  } else if (valid) {
     Spinor<R> o;
     hop<PS, PL, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
-    // per-RHS clover slot; a negative slot index means no clover term for
-    // that RHS (A = 1), so Wilson and clover systems can share a batch
-    const void* clov = a.clover;
-    if (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) {
-      if (a.clover_idx) {
-        const int ci = a.clover_idx[r];
-        clov = ci >= 0 ? static_cast<const char*>(a.clover) + a.clover_stride * (size_t)ci : nullptr;
-      }
-    }
+    const void* clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) ? clover_of(a, r) : nullptr;
     if (EPI & EPI_CPRE)
       if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
     if (EPI & EPI_XPAY) {
