@@ -229,7 +229,7 @@ int Engine::chunk_length() const {
       // restarts this step: the segment runs from |r_ne|^2 to delta^2 |r_ne|^2
       const double rt = rate_[r] < 0 ? rate_[r] : prior_rate_;
       nd = rt < 0 ? log(rp_.delta2) / rt : 4.0;
-      if (!fresh_[r]) nd = std::min(nd, (double)(P.maxiter - w.hi(I_ITERS)[r]));
+      nd = std::min(nd, (double)(P.maxiter - (fresh_[r] ? 0 : w.hi(I_ITERS)[r])));
     } else {
       if (w.hi(I_DONE)[r] || !w.hi(I_ACTIVE)[r]) continue;
       const double rr = w.hd(D_RR)[r], tr = w.hd(D_TRIG)[r];

@@ -175,10 +175,12 @@ QCU_D int word_of(const int4 w[3], int k) {
   return l == 0 ? c.x : (l == 1 ? c.y : (l == 2 ? c.z : c.w));
 }
 
-// h = P_mu psi of the 16-bit neighbour spinor, spin-paired and scaled by its
-// norm times `phase`. Same projector rows as project().
+// h = P_mu psi of the 16-bit neighbour spinor, spin-paired, in units of its
+// 16-bit grid; returns the scale (norm times `phase`) that the reconstruction
+// applies (the hop is linear, so scaling U h equals scaling h). Same projector
+// rows as project().
 template <int MU, bool FWD, int F>
-QCU_D void load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, float phase) {
+QCU_D float load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, float phase) {
   constexpr int S = FWD ? -F : F;
   constexpr float fS = (float)S;
   constexpr bool SWAP = (MU == 0 || MU == 1);  // lower pair as (p3, p2)
@@ -208,9 +210,10 @@ QCU_D void load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, f
       hre = ffma2(Qre, splat2(fS), Pre);
       him = ffma2(Qim, splat2(fS), Pim);
     }
-    h.re[c] = fmul2(hre, splat2(nm));
-    h.im[c] = fmul2(him, splat2(nm));
+    h.re[c] = hre;
+    h.im[c] = him;
   }
+  return nm;
 }
 
 // a = U h (FWD) or U^dag h, both spin components at once
@@ -240,27 +243,31 @@ QCU_D void su3_mul_pair(HalfPair& a, const Link<float>& U, const HalfPair& h) {
   }
 }
 
-// out += reconstruct(a), a spin-paired (lanes: U h0, U h1); same rows as reconstruct()
+// out += sc * reconstruct(a), a spin-paired (lanes: U h0, U h1); same rows as
+// reconstruct(), with the neighbour's scale folded into the sign factors
 template <int MU, bool FWD, int F>
-QCU_D void reconstruct_pair(SpinPair& o, const HalfPair& a) {
+QCU_D void reconstruct_pair(SpinPair& o, const HalfPair& a, float sc) {
   constexpr int S = FWD ? -F : F;
-  constexpr float fS = (float)S;
+  const float fS = (float)S * sc;
+  const float2 up = splat2(sc);
+  const float2 same = splat2(fS), nsame = splat2(-fS);
+  const float2 mixed = make_float2(-fS, fS), mixed_r = make_float2(fS, -fS);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    o.ure[c] = fadd2(o.ure[c], a.re[c]);
-    o.uim[c] = fadd2(o.uim[c], a.im[c]);
+    o.ure[c] = ffma2(a.re[c], up, o.ure[c]);
+    o.uim[c] = ffma2(a.im[c], up, o.uim[c]);
     if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a  ->  X = (o3, o2) -= S i (a, b)
-      o.xre[c] = ffma2(a.im[c], splat2(fS), o.xre[c]);
-      o.xim[c] = ffma2(a.re[c], splat2(-fS), o.xim[c]);
+      o.xre[c] = ffma2(a.im[c], same, o.xre[c]);
+      o.xim[c] = ffma2(a.re[c], nsame, o.xim[c]);
     } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a  ->  X += (-S a, S b)
-      o.xre[c] = ffma2(a.re[c], make_float2(-fS, fS), o.xre[c]);
-      o.xim[c] = ffma2(a.im[c], make_float2(-fS, fS), o.xim[c]);
+      o.xre[c] = ffma2(a.re[c], mixed, o.xre[c]);
+      o.xim[c] = ffma2(a.im[c], mixed, o.xim[c]);
     } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b  ->  L += (-S i a, S i b)
-      o.lre[c] = ffma2(a.im[c], make_float2(fS, -fS), o.lre[c]);
-      o.lim[c] = ffma2(a.re[c], make_float2(-fS, fS), o.lim[c]);
+      o.lre[c] = ffma2(a.im[c], mixed_r, o.lre[c]);
+      o.lim[c] = ffma2(a.re[c], mixed, o.lim[c]);
     } else {  // o2 += S a, o3 += S b
-      o.lre[c] = ffma2(a.re[c], splat2(fS), o.lre[c]);
-      o.lim[c] = ffma2(a.im[c], splat2(fS), o.lim[c]);
+      o.lre[c] = ffma2(a.re[c], same, o.lre[c]);
+      o.lim[c] = ffma2(a.im[c], same, o.lim[c]);
     }
   }
 }
@@ -271,13 +278,13 @@ QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, 
   Link<float> U;
   HalfPair h, a;
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
+  float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
   su3_mul_pair<true>(a, U, h);
-  reconstruct_pair<MU, true, F>(o, a);
+  reconstruct_pair<MU, true, F>(o, a, sc);
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
+  sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
   su3_mul_pair<false>(a, U, h);
-  reconstruct_pair<MU, false, F>(o, a);
+  reconstruct_pair<MU, false, F>(o, a, sc);
 }
 
 template <int PL, bool DAG>

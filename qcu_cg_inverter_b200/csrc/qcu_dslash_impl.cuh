@@ -45,6 +45,19 @@ constexpr int dslash_minb(int op, int epi) {
                                          : QCU_DSLASH_MINB;
 }
 
+// |v|^2 of one site: in the spinor's own precision (FP32 sums of 24 terms for
+// the sloppy operators, no per-term conversion to double), then FP64 across
+// sites in the block reduction
+template <class R> QCU_D double site_norm2(const Spinor<R>& v) {
+  R n = R(0);
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    n = fma(v.c[k].re, v.c[k].re, n);
+    n = fma(v.c[k].im, v.c[k].im, n);
+  }
+  return (double)n;
+}
+
 // Clover field of RHS r: its slot in the bank, or nullptr for a negative slot
 // index (no clover term for that RHS, A = 1), so Wilson and clover systems can
 // share a batch.
@@ -160,14 +173,10 @@ __global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const
       }
       SpinorIO<PA>::store(a.xacc, s, r, xv);
       SpinorIO<PA>::store(a.racc, s, r, rv);
-#pragma unroll
-      for (int k = 0; k < 12; k++) nrm += (double)rv.c[k].re * rv.c[k].re + (double)rv.c[k].im * rv.c[k].im;
+      nrm = site_norm2(rv);
     } else {
       SpinorIO<PS>::store(a.out, s, r, o);
-      if (EPI & EPI_NORM) {
-#pragma unroll
-        for (int k = 0; k < 12; k++) nrm += (double)o.c[k].re * o.c[k].re + (double)o.c[k].im * o.c[k].im;
-      }
+      if (EPI & EPI_NORM) nrm = site_norm2(o);
     }
     if (EPI & EPI_OUT2) {
       if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);

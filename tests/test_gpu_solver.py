@@ -135,6 +135,43 @@ def test_allocation_failure_is_reported(cuda, qcu_lib, oracle):
         assert rep["converged"]
 
 
+def test_iteration_cap_reports_not_converged(cuda, qcu_lib, oracle):
+    """A cap far below the iterations needed: every RHS stops at the cap with
+    status NOT_CONVERGED, the returned x is the FP64-checked iterate (its
+    reported true residual matches the oracle's), and the call raises only
+    when asked to."""
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 12, 0.4)
+    bs = np.stack([oracle.full_spinor_random(L, 30 + r) for r in range(3)])
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        xb = dev(np.zeros_like(bs))
+        reps = c.invert(xb, dev(bs), nrhs=3, kappas=[0.125, 0.13, 0.135], csw=1.0, tol=1e-10, maxiter=7,
+                        precision="half", raise_on_fail=False)
+        xs = host(xb, bs.shape)
+        for r, k in enumerate([0.125, 0.13, 0.135]):
+            rep = reps[r]
+            assert not rep["converged"] and rep["status"] == qcu_lib.QCU_ERR_NOT_CONVERGED
+            assert 7 <= rep["iterations"] <= 8
+            res = true_residual(oracle, xs[r], bs[r], U, L, k, 1.0)
+            assert 1e-10 < res < 1.0
+            assert abs(res - rep["true_residual"]) < 1e-6 * res
+        with pytest.raises(qcu_lib.QcuError) as e:
+            c.invert(dev(np.zeros_like(bs[0])), dev(bs[0]), kappa=0.13, csw=1.0, maxiter=5)
+        assert e.value.code == qcu_lib.QCU_ERR_NOT_CONVERGED
+
+
+def test_zero_source_converges_at_once(cuda, qcu_lib, oracle):
+    L = (8, 8, 8, 8)
+    b = np.zeros((2, 2048, 4, 3), complex)
+    with qcu_lib.Context(L) as c:
+        c.generate_gauge(3, 0.4)
+        x = dev(np.ones_like(b))
+        rep = c.invert(x, dev(b), kappa=0.13, csw=1.0)[0]
+        assert rep["converged"] and rep["iterations"] == 0
+        assert np.abs(host(x, b.shape)).max() == 0.0
+
+
 def test_kernel_launches_are_counted(cuda, qcu_lib):
     with qcu_lib.Context((8, 8, 8, 8)) as c:
         c.generate_gauge(1, 0.3)
