@@ -183,6 +183,38 @@ def cpu_oracle_solve(U, b, L, threads=None):
     return {"solve_s": time.perf_counter() - t0, "iterations": iters, "true_residual": res, "cores": O.num_threads()}
 
 
+def time_drop_in(ctx, torch, device, reps=20):
+    """The reference-signature entry points dslashQcu and fullDslashQcu on
+    device AoS buffers at the headline lattice, wall time per call (each call
+    is synchronous, as in the reference; the reference arm times the reference
+    library's own calls the same way)."""
+    import numpy as np
+
+    import qcu_cg_inverter_b200 as q
+    L, V = LATTICE, ctx.volume
+    U = np.zeros((4, 2, V // 2, 3, 3), complex)
+    ctx.export_gauge(U)
+    gauge = torch.from_numpy(U.reshape(-1)).to(device)
+    psi = torch.empty(V * 12, dtype=torch.complex128, device=device)
+    ctx.generate_spinor(psi, 1, SOURCE_SEED)
+    out = torch.zeros_like(psi)
+    half_in, half_out = psi[V * 6:].clone(), torch.zeros(V * 6, dtype=torch.complex128, device=device)
+    p = q.param(L)
+    q.initGridSize((1, 1, 1, 1), p, gauge, psi, out)
+    res = {"lattice": L}
+    for name, call in (("dslashQcu_ms", lambda: q.dslashQcu(half_out, half_in, gauge, p, 0)),
+                       ("fullDslashQcu_ms", lambda: q.fullDslashQcu(out, psi, gauge, p, 0))):
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            call()
+        torch.cuda.synchronize(device)
+        res[name] = (time.perf_counter() - t0) / reps * 1e3
+    return res
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -265,6 +297,7 @@ def run_ours(args, world, rank, local):
         achieved = nbytes / (ms / 1e3) / 1e9
         # in-solve kernel at the headline size (fields L2-resident)
         ms_small, nbytes_small = ctx.bench_stencil("half", 2, 1, 50)
+        drop_in = time_drop_in(ctx, torch, device)
         steps = args.steps
         per = t_mixed / steps
         out = {
@@ -295,6 +328,7 @@ def run_ours(args, world, rank, local):
                        "half_hop_GBps": bytes_hop16 / (ms_hop16 / 1e3) / 1e9,
                        "half_fused_GBps": achieved,
                        "in_solve_16x32_half_fused_GBps": nbytes_small / (ms_small / 1e3) / 1e9},
+            "drop_in": drop_in,
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -477,7 +511,7 @@ def run_serve(args):
     import qcu_cg_inverter_b200 as q
     device = torch.device("cuda", 0)
     srv = q.Server(0, columns=args.columns, clover_slots=args.clover_slots, tol=TOL, bc_t=BC_T,
-                   precision=q._PREC[args.precision])
+                   precision=q._PREC[args.precision], max_chunk=args.max_chunk)
     cids = {}
     for li, L in enumerate(SERVE_LATTICES):
         for c in range(3):
@@ -545,7 +579,8 @@ def run_serve(args):
                    "rate_per_s": SERVE_RATE, "kappa": [0.120, 0.1375], "csw": [0.0, 1.0], "nrhs": [1, 12],
                    "configs_per_lattice": 3, "eps": SERVE_EPS, "tol": TOL, "precision": args.precision,
                    "columns_per_config": args.columns, "clover_slots_per_config": args.clover_slots,
-                   "trace_seed": SERVE_SEED, "output_ring_per_lattice": args.out_ring},
+                   "trace_seed": SERVE_SEED, "output_ring_per_lattice": args.out_ring,
+                   "max_chunk": args.max_chunk},
         "e2e": {"h2d_bytes": h2d, "d2h_bytes": h2d},
         "device_bytes_resident": srv.device_bytes, "prepare_s": t_prep,
         "clocks": clk.summary(),
@@ -594,6 +629,7 @@ def main():
     ap.add_argument("--columns", type=int, default=16, help="--serve: RHS columns per resident configuration")
     ap.add_argument("--clover-slots", type=int, default=8, help="--serve: clover fields per configuration")
     ap.add_argument("--out-ring", type=int, default=4, help="--serve: pinned output buffers per lattice")
+    ap.add_argument("--max-chunk", type=int, default=8, help="--serve: most CG iterations between admissions")
     args = ap.parse_args()
     if args.serve:
         run_serve(args)

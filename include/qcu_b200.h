@@ -177,6 +177,7 @@ typedef struct {
   int clover_slots;         /* factored clover fields per resident configuration (8) */
   long long device_budget;  /* device bytes for resident configurations (0 = 85% of free memory) */
   int autotune;             /* tune launch shapes when a configuration becomes resident (1) */
+  int max_chunk;            /* most CG iterations between two admission points of a batch (8) */
 } qcu_server_params;
 
 void qcuServerParamsDefault(qcu_server_params* params);

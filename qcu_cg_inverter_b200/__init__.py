@@ -61,7 +61,8 @@ class SolveParams(ctypes.Structure):
 class ServerParams(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("tol", ctypes.c_double), ("maxiter", ctypes.c_int),
                 ("bc_t", ctypes.c_double), ("delta", ctypes.c_double), ("columns", ctypes.c_int),
-                ("clover_slots", ctypes.c_int), ("device_budget", ctypes.c_longlong), ("autotune", ctypes.c_int)]
+                ("clover_slots", ctypes.c_int), ("device_budget", ctypes.c_longlong), ("autotune", ctypes.c_int),
+                ("max_chunk", ctypes.c_int)]
 
 
 class SolveReport(ctypes.Structure):

@@ -241,7 +241,7 @@ int Engine::chunk_length() const {
     any = true;
   }
   if (!any) return 0;
-  return (int)std::max(1.0, std::min(ceil(need), 64.0));
+  return (int)std::max(1.0, std::min(ceil(need), (double)std::max(1, P.max_chunk)));
 }
 
 int Engine::step(bool* launched) {

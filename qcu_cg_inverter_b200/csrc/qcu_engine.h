@@ -29,6 +29,9 @@ struct EngineParams {
   int maxiter = 20000;
   bool clover = true;  // clover epilogues compiled into the iteration (per-column A = 1 when the slot is -1)
   bool graphs = true;
+  // most sloppy iterations per step; new RHS join and finished ones leave only
+  // between steps, so a server keeps steps short
+  int max_chunk = 64;
 };
 
 // One request: n consecutive columns with one kappa and one clover slot.

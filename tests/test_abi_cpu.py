@@ -83,6 +83,7 @@ def test_server_param_defaults(qcu_lib):
     sp = qcu_lib.server_params()
     assert sp.precision == qcu_lib.PREC_HALF and sp.tol == 1e-10 and sp.maxiter == 20000 and sp.bc_t == -1.0
     assert sp.columns == 16 and sp.clover_slots == 8 and sp.device_budget == 0 and sp.autotune == 1
+    assert sp.max_chunk == 8
 
 
 def test_server_entry_points_are_declared(qcu_lib):
