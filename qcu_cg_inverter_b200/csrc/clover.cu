@@ -322,25 +322,44 @@ __global__ void __launch_bounds__(256) clover_apply_kernel(Geom g, int parity, i
   }
 }
 
-// |A r|^2 (reduced per RHS) and u = A^-1 r, FP64, one read of r
-__global__ void __launch_bounds__(256) clover_res_kernel(Geom g, int parity, int nrhs, CSpinorView rin, SpinorView u,
-                                                         const void* A, const void* Ainv, size_t clov_stride,
-                                                         const int* clov_idx, const int* active, ReduceArgs red) {
+// |A r|^2 (reduced per RHS) and u = A^-1 r, FP64, one read of r. Works one
+// chiral block at a time (six components of r, one 6x6 block of A, then of
+// A^-1), so a thread holds one block and half a spinor.
+__global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, int nrhs, CSpinorView rin, SpinorView u,
+                                                            const void* A, const void* Ainv, size_t clov_stride,
+                                                            const int* clov_idx, const int* active, ReduceArgs red) {
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
   const bool valid = (s < g.Vh) && (r < nrhs) && (active == nullptr || active[r]);
   double nrm = 0.0;
   if (valid) {
-    Spinor<double> v, w;
-    SpinorIO<PREC_DOUBLE>::load(v, rin, s, r);
-    w = v;
-    const int ci = clov_idx ? clov_idx[r] : 0;
-    if (ci >= 0) {  // negative slot: A = 1
-      clover_apply_site<PREC_DOUBLE>(v, static_cast<const char*>(A) + clov_stride * (size_t)ci, g.Vh_pad, parity, s);
-      clover_apply_site<PREC_DOUBLE>(w, static_cast<const char*>(Ainv) + clov_stride * (size_t)ci, g.Vh_pad, parity, s);
+    const double2* rp = static_cast<const double2*>(rin.data);
+    double2* up = static_cast<double2*>(u.data);
+    const int ci = clov_idx ? clov_idx[r] : 0;  // negative slot: A = 1
+    const char* a = ci >= 0 ? static_cast<const char*>(A) + clov_stride * (size_t)ci : nullptr;
+    const char* ai = ci >= 0 ? static_cast<const char*>(Ainv) + clov_stride * (size_t)ci : nullptr;
+#pragma unroll 1
+    for (int b = 0; b < 2; b++) {
+      Cplx<double> v[6], w[6];
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        const double2 x = rp[chunk_index(6 * b + i, s, r, 12, rin.nrhs)];
+        v[i] = w[i] = mk(x.x, x.y);
+      }
+      if (a) {
+        HermBlock<double> B;
+        CloverIO<PREC_DOUBLE>::load_block(B, a, g.Vh_pad, parity, s, b);
+        herm_apply(B, v);
+        CloverIO<PREC_DOUBLE>::load_block(B, ai, g.Vh_pad, parity, s, b);
+        herm_apply(B, w);
+      }
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        nrm = fma(v[i].re, v[i].re, nrm);
+        nrm = fma(v[i].im, v[i].im, nrm);
+        up[chunk_index(6 * b + i, s, r, 12, u.nrhs)] = make_double2(w[i].re, w[i].im);
+      }
     }
-    SpinorIO<PREC_DOUBLE>::store(u, s, r, w);
-    for (int k = 0; k < 12; k++) nrm += v.c[k].re * v.c[k].re + v.c[k].im * v.c[k].im;
   }
   double vv[1] = {nrm};
   block_reduce_finish<1, FinNone>(vv, nrhs, red);
