@@ -47,9 +47,9 @@ KAPPA, CSW, EPS, BC_T, TOL = 0.1375, 1.0, 0.4, -1.0, 1e-10
 GAUGE_SEED, SOURCE_SEED = 20241, 7
 ROOF_LATTICE = (32, 32, 32, 64)
 # DRAM bytes (read + write) per output site of the fused 16-bit stencil,
-# from an ncu capture of one launch at 32^4 (612.9 MB for 524288 sites);
+# from an ncu capture of one launch at 32^4 (592.9 MB for 524288 sites);
 # the traffic grows with the number of sites, so a 32^3x64 launch moves twice that
-ROOF_TRAFFIC_BYTES_PER_SITE = 612.9e6 / 524288
+ROOF_TRAFFIC_BYTES_PER_SITE = 592.9e6 / 524288
 METRIC = "CG time to |r|/|b|<1e-10, mixed vs FP64 (16^3x32 Wilson-clover, kappa 0.1375, c_sw 1)"
 
 
