@@ -154,9 +154,9 @@ struct HalfPair {
   float2 re[3], im[3];
 };
 
-// Spin-paired accumulator: U = (o0, o1), L = (o2, o3), X = (o3, o2) (the
-// directions whose reconstruction pairs the lower spins in swapped order add
-// into X; L and X are combined once at the end).
+// Spin-paired accumulator: U = (o0, o1), L = (o2, o3), X = (o3, o2): the
+// directions whose reconstruction pairs the lower spins in swapped order (0
+// and 1) add into X, which is folded into L before directions 2 and 3.
 struct SpinPair {
   float2 ure[3], uim[3], lre[3], lim[3], xre[3], xim[3];
 };
@@ -292,12 +292,17 @@ QCU_D void hop_spin_pair(SpinPair& o, const Geom& g, int parity, int s, int r, c
                          const void* gauge, float bc_t) {
   constexpr int F = DAG ? -1 : 1;
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    o.ure[c] = o.uim[c] = o.lre[c] = o.lim[c] = o.xre[c] = o.xim[c] = make_float2(0.f, 0.f);
-  }
+  for (int c = 0; c < 3; c++) o.ure[c] = o.uim[c] = o.xre[c] = o.xim[c] = make_float2(0.f, 0.f);
   const Nbrs nb = neighbours(g, s, parity);
   hop_dir_pair<PL, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
   hop_dir_pair<PL, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  // only directions 0 and 1 add into X, only 2 and 3 into L: fold X into L
+  // now, so that the second half of the hop holds one lower accumulator
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.lre[c] = make_float2(o.xre[c].y, o.xre[c].x);
+    o.lim[c] = make_float2(o.xim[c].y, o.xim[c].x);
+  }
   hop_dir_pair<PL, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
   hop_dir_pair<PL, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
 }
@@ -311,8 +316,8 @@ QCU_D void hop_half_pair(Spinor<float>& out, const Geom& g, int parity, int s, i
   for (int c = 0; c < 3; c++) {
     out.c[c] = mk(o.ure[c].x, o.uim[c].x);
     out.c[3 + c] = mk(o.ure[c].y, o.uim[c].y);
-    out.c[6 + c] = mk(o.lre[c].x + o.xre[c].y, o.lim[c].x + o.xim[c].y);
-    out.c[9 + c] = mk(o.lre[c].y + o.xre[c].x, o.lim[c].y + o.xim[c].x);
+    out.c[6 + c] = mk(o.lre[c].x, o.lim[c].x);
+    out.c[9 + c] = mk(o.lre[c].y, o.lim[c].y);
   }
 }
 
@@ -335,10 +340,10 @@ QCU_D void hop_half_block(SpinBlock& out, const Geom& g, int parity, int s, int 
   hop_spin_pair<PL, DAG>(o, g, parity, s, r, in, gauge, bc_t);
 #pragma unroll
   for (int c = 0; c < 3; c++) {  // spin 0 and 2 of colour c, then spin 1 and 3
-    out.re[c] = make_float2(o.ure[c].x, o.lre[c].x + o.xre[c].y);
-    out.im[c] = make_float2(o.uim[c].x, o.lim[c].x + o.xim[c].y);
-    out.re[3 + c] = make_float2(o.ure[c].y, o.lre[c].y + o.xre[c].x);
-    out.im[3 + c] = make_float2(o.uim[c].y, o.lim[c].y + o.xim[c].x);
+    out.re[c] = make_float2(o.ure[c].x, o.lre[c].x);
+    out.im[c] = make_float2(o.uim[c].x, o.lim[c].x);
+    out.re[3 + c] = make_float2(o.ure[c].y, o.lre[c].y);
+    out.im[3 + c] = make_float2(o.uim[c].y, o.lim[c].y);
   }
 }
 
