@@ -216,37 +216,35 @@ QCU_D float load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, 
   return nm;
 }
 
-// a = U h (FWD) or U^dag h, both spin components at once
+// row i of a = U h (FWD) or U^dag h, both spin components at once
 template <bool FWD>
-QCU_D void su3_mul_pair(HalfPair& a, const Link<float>& U, const HalfPair& h) {
+QCU_D void su3_row_pair(float2& re, float2& im, const Link<float>& U, const HalfPair& h, int i) {
+  re = make_float2(0.f, 0.f);
+  im = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int i = 0; i < 3; i++) {
-    float2 re = make_float2(0.f, 0.f), im = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      const Cplx<float> u = FWD ? U.u[i * 3 + j] : U.u[j * 3 + i];
-      const float2 ur = splat2(u.re), ui = splat2(u.im);
-      if (FWD) {  // u h
-        re = ffma2(ur, h.re[j], re);
-        re = ffma2(fneg2(ui), h.im[j], re);
-        im = ffma2(ur, h.im[j], im);
-        im = ffma2(ui, h.re[j], im);
-      } else {  // conj(u) h
-        re = ffma2(ur, h.re[j], re);
-        re = ffma2(ui, h.im[j], re);
-        im = ffma2(ur, h.im[j], im);
-        im = ffma2(fneg2(ui), h.re[j], im);
-      }
+  for (int j = 0; j < 3; j++) {
+    const Cplx<float> u = FWD ? U.u[i * 3 + j] : U.u[j * 3 + i];
+    const float2 ur = splat2(u.re), ui = splat2(u.im);
+    if (FWD) {  // u h
+      re = ffma2(ur, h.re[j], re);
+      re = ffma2(fneg2(ui), h.im[j], re);
+      im = ffma2(ur, h.im[j], im);
+      im = ffma2(ui, h.re[j], im);
+    } else {  // conj(u) h
+      re = ffma2(ur, h.re[j], re);
+      re = ffma2(ui, h.im[j], re);
+      im = ffma2(ur, h.im[j], im);
+      im = ffma2(fneg2(ui), h.re[j], im);
     }
-    a.re[i] = re;
-    a.im[i] = im;
   }
 }
 
-// out += sc * reconstruct(a), a spin-paired (lanes: U h0, U h1); same rows as
-// reconstruct(), with the neighbour's scale folded into the sign factors
+// out += sc * reconstruct(U h) (or U^dag h), spin-paired (lanes: from h0,
+// from h1); same rows as reconstruct(), with the neighbour's scale folded
+// into the sign factors. Each colour row of the product is added in as soon
+// as it is formed, so only one row is live at a time.
 template <int MU, bool FWD, int F>
-QCU_D void reconstruct_pair(SpinPair& o, const HalfPair& a, float sc) {
+QCU_D void mul_reconstruct_pair(SpinPair& o, const Link<float>& U, const HalfPair& h, float sc) {
   constexpr int S = FWD ? -F : F;
   const float fS = (float)S * sc;
   const float2 up = splat2(sc);
@@ -254,20 +252,22 @@ QCU_D void reconstruct_pair(SpinPair& o, const HalfPair& a, float sc) {
   const float2 mixed = make_float2(-fS, fS), mixed_r = make_float2(fS, -fS);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    o.ure[c] = ffma2(a.re[c], up, o.ure[c]);
-    o.uim[c] = ffma2(a.im[c], up, o.uim[c]);
+    float2 are, aim;
+    su3_row_pair<FWD>(are, aim, U, h, c);
+    o.ure[c] = ffma2(are, up, o.ure[c]);
+    o.uim[c] = ffma2(aim, up, o.uim[c]);
     if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a  ->  X = (o3, o2) -= S i (a, b)
-      o.xre[c] = ffma2(a.im[c], same, o.xre[c]);
-      o.xim[c] = ffma2(a.re[c], nsame, o.xim[c]);
+      o.xre[c] = ffma2(aim, same, o.xre[c]);
+      o.xim[c] = ffma2(are, nsame, o.xim[c]);
     } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a  ->  X += (-S a, S b)
-      o.xre[c] = ffma2(a.re[c], mixed, o.xre[c]);
-      o.xim[c] = ffma2(a.im[c], mixed, o.xim[c]);
+      o.xre[c] = ffma2(are, mixed, o.xre[c]);
+      o.xim[c] = ffma2(aim, mixed, o.xim[c]);
     } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b  ->  L += (-S i a, S i b)
-      o.lre[c] = ffma2(a.im[c], mixed_r, o.lre[c]);
-      o.lim[c] = ffma2(a.re[c], mixed, o.lim[c]);
+      o.lre[c] = ffma2(aim, mixed_r, o.lre[c]);
+      o.lim[c] = ffma2(are, mixed, o.lim[c]);
     } else {  // o2 += S a, o3 += S b
-      o.lre[c] = ffma2(a.re[c], same, o.lre[c]);
-      o.lim[c] = ffma2(a.im[c], same, o.lim[c]);
+      o.lre[c] = ffma2(are, same, o.lre[c]);
+      o.lim[c] = ffma2(aim, same, o.lim[c]);
     }
   }
 }
@@ -276,15 +276,13 @@ template <int PL, int MU, int F>
 QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, int s, int r, const CSpinorView& in,
                         const void* gauge, float bc_t) {
   Link<float> U;
-  HalfPair h, a;
+  HalfPair h;
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
   float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
-  su3_mul_pair<true>(a, U, h);
-  reconstruct_pair<MU, true, F>(o, a, sc);
+  mul_reconstruct_pair<MU, true, F>(o, U, h, sc);
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
   sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
-  su3_mul_pair<false>(a, U, h);
-  reconstruct_pair<MU, false, F>(o, a, sc);
+  mul_reconstruct_pair<MU, false, F>(o, U, h, sc);
 }
 
 template <int PL, bool DAG>

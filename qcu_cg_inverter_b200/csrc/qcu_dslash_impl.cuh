@@ -37,8 +37,13 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_MINB16_CGXR
 #define QCU_DSLASH_MINB16_CGXR 2
 #endif
+// whether the single-RHS 16-bit kernels take the same caps as the batched ones
+// (measured: no; 16^3x32 solve 3.88 vs 3.63 ms, 32^4 fused stencil 121 vs 114 us)
+#ifndef QCU_DSLASH_CAP_1RHS
+#define QCU_DSLASH_CAP_1RHS 0
+#endif
 constexpr int dslash_minb(int op, int epi) {
-  return (op_spinor_prec(op) != PREC_HALF || op == OP_HALF_FAST_1) ? QCU_DSLASH_MINB
+  return (op_spinor_prec(op) != PREC_HALF || (op == OP_HALF_FAST_1 && !QCU_DSLASH_CAP_1RHS)) ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
          : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
          : (epi == EPI_CPRE)             ? QCU_DSLASH_MINB16_CPRE
