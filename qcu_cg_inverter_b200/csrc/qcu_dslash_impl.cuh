@@ -42,8 +42,15 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_CAP_1RHS
 #define QCU_DSLASH_CAP_1RHS 0
 #endif
+// FP64 stencils (the FP64 solver and every reliable update): no register cap
+// beyond the 255 of the architecture, since the cap of 128 made them spill
+// (measured: FP64 hop at 32^3x64 249 -> 216 us; FP64 16^3x32 solve 7.21 -> 6.91 ms)
+#ifndef QCU_DSLASH_MINB64
+#define QCU_DSLASH_MINB64 1
+#endif
 constexpr int dslash_minb(int op, int epi) {
-  return (op_spinor_prec(op) != PREC_HALF || (op == OP_HALF_FAST_1 && !QCU_DSLASH_CAP_1RHS)) ? QCU_DSLASH_MINB
+  return op == OP_DOUBLE ? QCU_DSLASH_MINB64
+         : (op_spinor_prec(op) != PREC_HALF || (op == OP_HALF_FAST_1 && !QCU_DSLASH_CAP_1RHS)) ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
          : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
          : (epi == EPI_CPRE)             ? QCU_DSLASH_MINB16_CPRE
