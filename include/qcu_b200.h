@@ -241,6 +241,19 @@ qcu_context qcuLegacyContext(void);
  * allocations the next one fails as out-of-memory (n < 0 disables). */
 void qcuDebugFailAllocAfter(long long n);
 
+/* Test hook: one launch of the batched stencil with epilogue flags `epi`
+ * (1 A^-1 after the hop, 2 xpay, 4 A^-1 on x, 8 A^-1 after the xpay, 16 second
+ * output A^-1 y, 32 per-RHS norm, 64 CG x/r update) on fields converted from
+ * FP64 AoS spinors (nrhs x Vh x 12 complex, host or device memory; parity 0
+ * output). csw_eff[r] <= 0 means no clover term for RHS r. out, out2, xacc
+ * and racc are read before and written after the launch; norms[r] receives
+ * the launch's per-RHS sums. rhs_pairs: 1 = RHS-paired kernels, 0 = one RHS
+ * per thread, -1 = as built. */
+int qcuDebugStencil(qcu_context ctx, int precision, int dagger, int epi, int nrhs, const double* csw_eff,
+                    const double* coef, const double* alpha, const int* active, const void* in, const void* x,
+                    const void* pvec, void* out, void* out2, void* xacc, void* racc, double* norms,
+                    int rhs_pairs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -128,6 +128,8 @@ def lib():
                               ctypes.POINTER(SolveReport)]),
             "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
             "qcuDebugFailAllocAfter": (None, [ll]),
+            "qcuDebugStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d),
+                                    ctypes.POINTER(i), P, P, P, P, P, P, P, ctypes.POINTER(d), i]),
             "qcuAutotune": (i, [P, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(d)]),
             "qcuServerParamsDefault": (None, [ctypes.POINTER(ServerParams)]),
             "qcuServerCreate": (i, [ctypes.POINTER(P), i, ctypes.POINTER(ServerParams)]),
@@ -344,6 +346,26 @@ class Context:
         _check(lib().qcuBenchStencil(self._h, _PREC[precision], int(variant), int(nrhs), int(iters),
                                      ctypes.byref(ms), ctypes.byref(nbytes)))
         return ms.value, nbytes.value
+
+    def debug_stencil(self, precision, dagger: int, epi: int, inp, csw_eff, coef, active=None, x=None,
+                      out=None, out2=None, pvec=None, xacc=None, racc=None, alpha=None, rhs_pairs: int = -1):
+        """One batched stencil launch (epilogue flags `epi`) on fields converted
+        from the FP64 AoS arrays given (numpy, nrhs x Vh x 4 x 3 complex, parity
+        0 output); out/out2/xacc/racc are updated in place. rhs_pairs picks the
+        kernel family of the fast 16-bit operator (1 paired, 0 one RHS per
+        thread, -1 as built). Returns the per-RHS norms of the launch."""
+        import numpy as np
+        nrhs = len(csw_eff)
+        arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.complex128)
+        inp, x, out, out2, pvec, xacc, racc = map(arr, (inp, x, out, out2, pvec, xacc, racc))
+        ptr = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+        dv = lambda v: None if v is None else (ctypes.c_double * nrhs)(*[float(t) for t in v])
+        act = None if active is None else (ctypes.c_int * nrhs)(*[int(bool(t)) for t in active])
+        norms = (ctypes.c_double * nrhs)()
+        _check(lib().qcuDebugStencil(self._h, _PREC[precision], int(dagger), int(epi), nrhs, dv(csw_eff), dv(coef),
+                                     dv(alpha), act, ptr(inp), ptr(x), ptr(pvec), ptr(out), ptr(out2), ptr(xacc),
+                                     ptr(racc), norms, int(rhs_pairs)))
+        return dict(out=out, out2=out2, xacc=xacc, racc=racc, norms=np.array(list(norms)))
 
     def set_shape(self, rhs_lanes: int, site_lanes: int):
         """Thread-block shape (RHS lanes x site lanes) of single-RHS kernels."""

@@ -94,6 +94,10 @@ void PinnedBuf::release() {
 
 int Field::alloc(int prec_, int nsites_, int nrhs_, int nparity_, cudaStream_t st) {
   if (prec == prec_ && nsites == nsites_ && nrhs == nrhs_ && nparity == nparity_ && data.p) return QCU_SUCCESS;
+  if (!field_index32_ok(nsites_, nrhs_)) {
+    set_error(QCU_ERR_INVALID_ARG, "too many right-hand sides for this lattice (a field must hold < 2^32 chunks)");
+    return QCU_ERR_INVALID_ARG;
+  }
   prec = prec_;
   nsites = nsites_;
   nrhs = nrhs_;

@@ -1,4 +1,5 @@
-// qcuBenchStencil (device timing of the fused stencil on resident fields) and
+// qcuBenchStencil (device timing of the fused stencil on resident fields),
+// qcuDebugStencil (one stencil launch on converted fields, for tests) and
 // qcuExportGauge.
 #include <string.h>
 
@@ -119,5 +120,132 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
     int tiles = (nrhs + sh.Rb - 1) / sh.Rb;
     *bytes = (double)g.Vh * (nrhs * per_rhs + tiles * shared);
   }
+  return QCU_SUCCESS;
+}
+
+// One launch of a batched stencil on internal fields converted from AoS
+// spinors (FP64, nrhs x Vh x 12 complex each): the comparison point of the
+// kernel families against each other and against the CPU operator.
+extern "C" int qcuDebugStencil(qcu_context ctx, int prec, int dagger, int epi, int nrhs, const double* csw_eff,
+                               const double* coef, const double* alpha, const int* active, const void* in,
+                               const void* x, const void* pvec, void* out, void* out2, void* xacc, void* racc,
+                               double* norms, int rhs_pairs) {
+  clear_error();
+  QCU_CHECK(ctx_check(ctx));
+  const int known = EPI_CPRE | EPI_XPAY | EPI_CX | EPI_CPOST | EPI_OUT2 | EPI_NORM | EPI_CGXR;
+  const bool cgxr = (epi & EPI_CGXR) != 0;
+  if (prec < 0 || prec > 2 || nrhs < 1 || (epi & ~known) || !csw_eff || !coef || !in ||
+      ((epi & EPI_XPAY) && !x) || (!cgxr && !out) || ((epi & EPI_OUT2) && !out2) ||
+      (cgxr && (!xacc || !racc || !pvec || !alpha)) || rhs_pairs < -1 || rhs_pairs > 1) {
+    set_error(QCU_ERR_INVALID_ARG, "bad stencil arguments");
+    return QCU_ERR_INVALID_ARG;
+  }
+  if (!ctx->gauge_loaded) {
+    set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
+    return QCU_ERR_NOT_INITIALIZED;
+  }
+  const Geom& g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  const int op = ctx_op(ctx, prec);
+  const int ps = op_spinor_prec(op);
+  const int pa = ps == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE;
+  const size_t per = (size_t)g.Vh * 12;  // complex numbers per AoS spinor
+  const size_t aos_bytes = per * 16 * nrhs;
+  Field fin, fx, fp, fout, fout2, fxa, fra;
+  DevBuf aos, dcoef, dalpha, dact, dcidx;
+  QCU_CHECK(aos.ensure(aos_bytes, st));
+  auto ingest = [&](Field& f, int fp_prec, const void* src) -> int {
+    QCU_CHECK(f.alloc(fp_prec, g.Vh_pad, nrhs, 1, st));
+    QCU_CHECK_CUDA(cudaMemcpyAsync(aos.p, src, aos_bytes, cudaMemcpyDefault, st));
+    QCU_CHECK_CUDA(launch_spinor_in(fp_prec, g, nrhs, aos.p, per, f.view(0), st));
+    return QCU_SUCCESS;
+  };
+  auto egress = [&](const Field& f, void* dst) -> int {
+    QCU_CHECK_CUDA(launch_spinor_out(f.prec, g, nrhs, f.cview(0), aos.p, per, st));
+    QCU_CHECK_CUDA(cudaMemcpyAsync(dst, aos.p, aos_bytes, cudaMemcpyDefault, st));
+    return QCU_SUCCESS;
+  };
+  QCU_CHECK(ingest(fin, ps, in));
+  if (epi & EPI_XPAY) QCU_CHECK(ingest(fx, ps, x));
+  if (cgxr) {
+    QCU_CHECK(ingest(fp, ps, pvec));
+    QCU_CHECK(ingest(fxa, pa, xacc));
+    QCU_CHECK(ingest(fra, pa, racc));
+  } else {
+    QCU_CHECK(ingest(fout, ps, out));
+  }
+  if (epi & EPI_OUT2) QCU_CHECK(ingest(fout2, ps, out2));
+  // per-RHS clover fields (csw_eff <= 0: none), pinned while later values are
+  // built so that none evicts another; coefficients and mask
+  std::vector<int> cidx(nrhs, -1), act(nrhs, 1);
+  auto unpin = [&]() {
+    for (int r = 0; r < nrhs; r++)
+      if (cidx[r] >= 0 && ctx->clover.pinned[cidx[r]] > 0) ctx->clover.pinned[cidx[r]] -= 1;
+  };
+  for (int r = 0; r < nrhs; r++) {
+    if (csw_eff[r] > 0.0) {
+      const int st_slot = ctx_clover_slot(ctx, csw_eff[r], &cidx[r]);
+      if (st_slot != QCU_SUCCESS) {
+        cidx[r] = -1;
+        unpin();
+        return st_slot;
+      }
+      ctx->clover.pinned[cidx[r]] += 1;
+    }
+    if (active) act[r] = active[r] != 0;
+  }
+  unpin();  // every value is built; the launch below reads them in order
+  QCU_CHECK(dcoef.ensure(sizeof(double) * nrhs, st));
+  QCU_CHECK(dalpha.ensure(sizeof(double) * nrhs, st));
+  QCU_CHECK(dact.ensure(sizeof(int) * nrhs, st));
+  QCU_CHECK(dcidx.ensure(sizeof(int) * nrhs, st));
+  QCU_CHECK_CUDA(cudaMemcpyAsync(dcoef.p, coef, sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+  if (alpha) QCU_CHECK_CUDA(cudaMemcpyAsync(dalpha.p, alpha, sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+  QCU_CHECK_CUDA(cudaMemcpyAsync(dact.p, act.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+  QCU_CHECK_CUDA(cudaMemcpyAsync(dcidx.p, cidx.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+  const LaunchShape sh = ctx_shape(ctx, op, nrhs);
+  QCU_CHECK(ctx->red.ensure(g, nrhs, st, sh.Sb));
+  DslashArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = g;
+  a.parity = 0;
+  a.nrhs = nrhs;
+  a.in = fin.cview(0);
+  if (!cgxr) a.out = fout.view(0);
+  if (epi & EPI_XPAY) a.x = fx.cview(0);
+  if (epi & EPI_OUT2) a.out2 = fout2.view(0);
+  a.gauge = ctx_gauge(ctx, op);
+  a.clover = ctx_clover_ptr(ctx, op, true);
+  a.clover_stride = ctx_clover_stride(ctx, op);
+  a.clover_idx = dcidx.as<int>();
+  a.coef = dcoef.as<double>();
+  a.bc_t = -1.0;
+  a.active = dact.as<int>();
+  a.red = ctx->red.args();
+  if (cgxr) {
+    a.xacc = fxa.view(0);
+    a.racc = fra.view(0);
+    a.pvec = fp.cview(0);
+    a.alpha = dalpha.as<double>();
+  }
+  set_rhs_pairs_override(rhs_pairs);
+  const cudaError_t e = launch_dslash(op, dagger != 0, epi, FIN_NONE, a, sh, st);
+  set_rhs_pairs_override(-1);
+  if (e == cudaErrorInvalidValue) {
+    set_error(QCU_ERR_INVALID_ARG, "no stencil kernel for this epilogue");
+    return QCU_ERR_INVALID_ARG;
+  }
+  QCU_CHECK_CUDA(e);
+  ctx->launches++;
+  if (cgxr) {
+    QCU_CHECK(egress(fxa, xacc));
+    QCU_CHECK(egress(fra, racc));
+  } else {
+    QCU_CHECK(egress(fout, out));
+  }
+  if (epi & EPI_OUT2) QCU_CHECK(egress(fout2, out2));
+  if (norms && (epi & (EPI_NORM | EPI_CGXR)))
+    QCU_CHECK_CUDA(cudaMemcpyAsync(norms, ctx->red.result.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, st));
+  QCU_CHECK_CUDA(cudaStreamSynchronize(st));
   return QCU_SUCCESS;
 }

@@ -10,21 +10,60 @@ DslashKernelFn pick_f32(bool dag, int epi, int fin);
 DslashKernelFn pick_f16(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x1(bool dag, int epi, int fin);
+DslashKernelFn pick_f16p(bool dag, int epi, int fin);
+DslashKernelFn pick_f64b(bool dag, int epi, int fin);
+
+// Batched FP64 launches on their own kernel family (OP_DOUBLE_BATCH: capped,
+// row-at-a-time reconstruction) (1) or on the single-RHS one (0).
+#ifndef QCU_F64_BATCH
+#define QCU_F64_BATCH 1
+#endif
+
+// Batched launches of the fast 16-bit operator on the RHS-paired kernels (1)
+// or on one RHS per thread (0).
+#ifndef QCU_RHS_PAIRS
+#define QCU_RHS_PAIRS 1
+#endif
+// The CG update stencil (EPI_CGXR: hop, xpay, x and r in FP32) stays on one
+// RHS per thread unless this is 1. Measured in the 48-RHS 24^3x48 solve:
+// 0.519 s with it on one RHS per thread, 0.528 s paired (loads grouped by
+// three chunks), 0.546 s paired with one chunk at a time.
+#ifndef QCU_PAIR_CGXR
+#define QCU_PAIR_CGXR 0
+#endif
+
+static int g_pairs_override = -1;
+void set_rhs_pairs_override(int v) { g_pairs_override = v; }
 
 cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape sh,
                           cudaStream_t stream) {
+  const bool pairs = g_pairs_override < 0 ? QCU_RHS_PAIRS != 0 : g_pairs_override != 0;
+  const bool pair_cgxr = g_pairs_override < 0 ? QCU_PAIR_CGXR != 0 : g_pairs_override != 0;
   DslashKernelFn fn = nullptr;
+  // RHS lanes per thread: the RHS-paired kernels take a block of Rb/2 x Sb
+  // threads for the same Rb x Sb tile of (RHS, site)
+  int per_thread = 1;
   switch (prec) {
-    case PREC_DOUBLE: fn = pick_f64(dagger, epi, fin); break;
+    case PREC_DOUBLE: fn = (QCU_F64_BATCH && a.nrhs > 1) ? pick_f64b(dagger, epi, fin) : pick_f64(dagger, epi, fin); break;
     case PREC_SINGLE: fn = pick_f32(dagger, epi, fin); break;
     case PREC_HALF: fn = pick_f16(dagger, epi, fin); break;
-    case OP_HALF_FAST: fn = a.nrhs == 1 ? pick_f16x1(dagger, epi, fin) : pick_f16x(dagger, epi, fin); break;
+    case OP_HALF_FAST:
+      if (a.nrhs == 1) {
+        fn = pick_f16x1(dagger, epi, fin);
+      } else if (pairs && sh.Rb >= 2 && (pair_cgxr || !(epi & EPI_CGXR))) {
+        fn = pick_f16p(dagger, epi, fin);
+        per_thread = 2;
+      } else {
+        fn = pick_f16x(dagger, epi, fin);
+      }
+      break;
     default: break;
   }
   if (!fn) return cudaErrorInvalidValue;
-  if (sh.Rb < 1 || sh.Rb > 32 || (32 % sh.Rb) != 0 || (sh.Rb * sh.Sb) % 32 != 0 || sh.Rb * sh.Sb > 256)
+  const int tx = sh.Rb / per_thread;
+  if (sh.Rb < 1 || sh.Rb > 32 || (32 % sh.Rb) != 0 || (tx * sh.Sb) % 32 != 0 || sh.Rb * sh.Sb > 256)
     return cudaErrorInvalidConfiguration;
-  dim3 block(sh.Rb, sh.Sb);
+  dim3 block(tx, sh.Sb);
   dim3 grid(grid_x(a.g.Vh, sh.Sb), (a.nrhs + sh.Rb - 1) / sh.Rb);
   fn<<<grid, block, 0, stream>>>(a);
   return cudaGetLastError();

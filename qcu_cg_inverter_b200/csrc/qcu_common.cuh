@@ -164,8 +164,30 @@ QCU_HD Nbrs neighbours(const Geom& g, int s, int parity) {
 //     chunk(c, s, r) = ((s/32 * NC + c) * 32 + s%32) * nrhs + r
 // so a warp reading chunk c of 32 consecutive sites reads 512*nrhs contiguous
 // bytes, and all chunks of a site block sit within a few KB.
+//
+// Kernels compute the index in 32-bit unsigned arithmetic (the pointer add
+// then takes one wide multiply-add), so a field holds fewer than 2^32 chunks
+// per parity block: field_index32_ok is checked wherever fields are sized.
 QCU_HD size_t chunk_index(int c, int s, int r, int NC, int nrhs) {
+#ifdef __CUDA_ARCH__
+  return (((((unsigned)s >> 5) * (unsigned)NC + (unsigned)c) << 5) + ((unsigned)s & 31u)) * (unsigned)nrhs + (unsigned)r;
+#else
   return ((size_t)((s >> 5) * NC + c) * 32 + (s & 31)) * (size_t)nrhs + r;
+#endif
+}
+// per-site, per-RHS scalars (16-bit spinor norms)
+QCU_HD size_t site_rhs_index(int s, int r, int nrhs) {
+#ifdef __CUDA_ARCH__
+  return (unsigned)s * (unsigned)nrhs + (unsigned)r;
+#else
+  return (size_t)s * nrhs + r;
+#endif
+}
+// the largest chunk count per site of any field (FP64 clover: 36; FP64
+// spinors: 12 per RHS)
+inline bool field_index32_ok(long long Vh_pad, long long nrhs) {
+  const long long per_site = 12 * nrhs > 36 ? 12 * nrhs : 36;
+  return Vh_pad > 0 && nrhs > 0 && Vh_pad * per_site < (1LL << 32);
 }
 
 // ---------------------------------------------------------------------------
@@ -188,11 +210,20 @@ enum OpVariant : int {
   // the same storage as OP_HALF_FAST; the kernels its launches use for a
   // single RHS (block-paired epilogues at 128 registers)
   OP_HALF_FAST_1 = 4,
+  // the same storage again; the kernels of its batched launches: two
+  // right-hand sides per thread in the lanes of paired FP32 instructions
+  OP_HALF_FAST_2 = 5,
+  // the storage of OP_DOUBLE; the kernels of its batched launches (a register
+  // cap and row-at-a-time reconstruction)
+  OP_DOUBLE_BATCH = 6,
 };
-__host__ __device__ constexpr bool op_fast(int op) { return op == OP_HALF_FAST || op == OP_HALF_FAST_1; }
-__host__ __device__ constexpr int op_spinor_prec(int op) { return op_fast(op) ? (int)PREC_HALF : op; }
-__host__ __device__ constexpr int op_link_format(int op) { return op_fast(op) ? (int)LINK_SINGLE18 : op; }
-__host__ __device__ constexpr int op_clover_prec(int op) { return op_fast(op) ? (int)PREC_SINGLE : op; }
+__host__ __device__ constexpr bool op_fast(int op) {
+  return op == OP_HALF_FAST || op == OP_HALF_FAST_1 || op == OP_HALF_FAST_2;
+}
+__host__ __device__ constexpr int op_base(int op) { return op == OP_DOUBLE_BATCH ? (int)OP_DOUBLE : op; }
+__host__ __device__ constexpr int op_spinor_prec(int op) { return op_fast(op) ? (int)PREC_HALF : op_base(op); }
+__host__ __device__ constexpr int op_link_format(int op) { return op_fast(op) ? (int)LINK_SINGLE18 : op_base(op); }
+__host__ __device__ constexpr int op_clover_prec(int op) { return op_fast(op) ? (int)PREC_SINGLE : op_base(op); }
 
 // 16-bit storage is fixed point: a real v in [-1,1] is stored as
 // round(v*32767); spinors and clover blocks carry one float norm per site so

@@ -42,49 +42,82 @@ QCU_D void project(Half2<R>& h, const Spinor<R>& p) {
   }
 }
 
-// out += reconstruct(a = U h0, b = U h1)
+// out += reconstruct(a = U h0, b = U h1), colour row c
 template <int MU, bool FWD, int F, class R>
-QCU_D void reconstruct(Spinor<R>& o, const Cplx<R> a[3], const Cplx<R> b[3]) {
+QCU_D void reconstruct_row(Spinor<R>& o, int c, const Cplx<R>& a, const Cplx<R>& b) {
   constexpr int S = FWD ? -F : F;  // same sign convention as project()
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    o.c[c] += a[c];
-    o.c[3 + c] += b[c];
-    if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a
-      if (S > 0) { o.c[6 + c] -= mul_i(b[c]); o.c[9 + c] -= mul_i(a[c]); }
-      else { o.c[6 + c] += mul_i(b[c]); o.c[9 + c] += mul_i(a[c]); }
-    } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a
-      if (S > 0) { o.c[6 + c] += b[c]; o.c[9 + c] -= a[c]; }
-      else { o.c[6 + c] -= b[c]; o.c[9 + c] += a[c]; }
-    } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b
-      if (S > 0) { o.c[6 + c] -= mul_i(a[c]); o.c[9 + c] += mul_i(b[c]); }
-      else { o.c[6 + c] += mul_i(a[c]); o.c[9 + c] -= mul_i(b[c]); }
-    } else {  // o2 += S a, o3 += S b
-      if (S > 0) { o.c[6 + c] += a[c]; o.c[9 + c] += b[c]; }
-      else { o.c[6 + c] -= a[c]; o.c[9 + c] -= b[c]; }
-    }
+  o.c[c] += a;
+  o.c[3 + c] += b;
+  if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a
+    if (S > 0) { o.c[6 + c] -= mul_i(b); o.c[9 + c] -= mul_i(a); }
+    else { o.c[6 + c] += mul_i(b); o.c[9 + c] += mul_i(a); }
+  } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a
+    if (S > 0) { o.c[6 + c] += b; o.c[9 + c] -= a; }
+    else { o.c[6 + c] -= b; o.c[9 + c] += a; }
+  } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b
+    if (S > 0) { o.c[6 + c] -= mul_i(a); o.c[9 + c] += mul_i(b); }
+    else { o.c[6 + c] += mul_i(a); o.c[9 + c] -= mul_i(b); }
+  } else {  // o2 += S a, o3 += S b
+    if (S > 0) { o.c[6 + c] += a; o.c[9 + c] += b; }
+    else { o.c[6 + c] -= a; o.c[9 + c] -= b; }
   }
 }
+template <int MU, bool FWD, int F, class R>
+QCU_D void reconstruct(Spinor<R>& o, const Cplx<R> a[3], const Cplx<R> b[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) reconstruct_row<MU, FWD, F>(o, c, a[c], b[c]);
+}
 
+// row i of U v and of U^dag v
+template <class R>
+QCU_D Cplx<R> su3_row(const Link<R>& U, const Cplx<R> v[3], int i) {
+  Cplx<R> acc = U.u[i * 3] * v[0];
+  cmac(acc, U.u[i * 3 + 1], v[1]);
+  cmac(acc, U.u[i * 3 + 2], v[2]);
+  return acc;
+}
+template <class R>
+QCU_D Cplx<R> su3_dag_row(const Link<R>& U, const Cplx<R> v[3], int i) {
+  Cplx<R> acc = mk(R(0), R(0));
+  cmac_conj(acc, U.u[i], v[0]);
+  cmac_conj(acc, U.u[3 + i], v[1]);
+  cmac_conj(acc, U.u[6 + i], v[2]);
+  return acc;
+}
 template <class R>
 QCU_D void su3_mul(Cplx<R> o[3], const Link<R>& U, const Cplx<R> v[3]) {
 #pragma unroll
-  for (int i = 0; i < 3; i++) {
-    Cplx<R> acc = U.u[i * 3] * v[0];
-    cmac(acc, U.u[i * 3 + 1], v[1]);
-    cmac(acc, U.u[i * 3 + 2], v[2]);
-    o[i] = acc;
-  }
+  for (int i = 0; i < 3; i++) o[i] = su3_row(U, v, i);
 }
 template <class R>
 QCU_D void su3_dag_mul(Cplx<R> o[3], const Link<R>& U, const Cplx<R> v[3]) {
 #pragma unroll
-  for (int i = 0; i < 3; i++) {
-    Cplx<R> acc = mk(R(0), R(0));
-    cmac_conj(acc, U.u[i], v[0]);
-    cmac_conj(acc, U.u[3 + i], v[1]);
-    cmac_conj(acc, U.u[6 + i], v[2]);
-    o[i] = acc;
+  for (int i = 0; i < 3; i++) o[i] = su3_dag_row(U, v, i);
+}
+
+// out += reconstruct(U h) (FWD) or reconstruct(U^dag h). ROWS: each colour row
+// of the products is added in as soon as it is formed (fewer live registers;
+// the same operations): faster for batched FP64 launches at a 128-register
+// cap, slower for single-RHS ones without a cap.
+template <int MU, bool FWD, int F, bool ROWS, class R>
+QCU_D void mul_reconstruct(Spinor<R>& o, const Link<R>& U, const Half2<R>& h) {
+  if constexpr (ROWS) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const Cplx<R> a = FWD ? su3_row(U, h.h0, i) : su3_dag_row(U, h.h0, i);
+      const Cplx<R> b = FWD ? su3_row(U, h.h1, i) : su3_dag_row(U, h.h1, i);
+      reconstruct_row<MU, FWD, F>(o, i, a, b);
+    }
+  } else {
+    Cplx<R> a[3], b[3];
+    if (FWD) {
+      su3_mul(a, U, h.h0);
+      su3_mul(b, U, h.h1);
+    } else {
+      su3_dag_mul(a, U, h.h0);
+      su3_dag_mul(b, U, h.h1);
+    }
+    reconstruct<MU, FWD, F>(o, a, b);
   }
 }
 
@@ -119,24 +152,19 @@ QCU_D void load_project(Half2<R>& h, const CSpinorView& in, int s, int r, R phas
 
 // One direction (both hops) of the stencil: PS = spinor precision, PL = link
 // storage format.
-template <int PS, int PL, int MU, int F, class R>
+template <int PS, int PL, int MU, int F, bool ROWS, class R>
 QCU_D void hop_dir(Spinor<R>& o, const Geom& g, const Nbrs& nb, int parity, int s, int r,
                    const CSpinorView& in, const void* gauge, R bc_t) {
   Link<R> U;
   Half2<R> h;
-  Cplx<R> a[3], b[3];
   // forward: U_mu(x) in(x+mu)
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
   load_project<PS, MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : R(1));
-  su3_mul(a, U, h.h0);
-  su3_mul(b, U, h.h1);
-  reconstruct<MU, true, F>(o, a, b);
+  mul_reconstruct<MU, true, F, ROWS>(o, U, h);
   // backward: U_mu(x-mu)^dag in(x-mu); the link lives on the other parity
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
   load_project<PS, MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : R(1));
-  su3_dag_mul(a, U, h.h0);
-  su3_dag_mul(b, U, h.h1);
-  reconstruct<MU, false, F>(o, a, b);
+  mul_reconstruct<MU, false, F, ROWS>(o, U, h);
 }
 
 // ---------------------------------------------------------------------------
@@ -188,7 +216,7 @@ QCU_D float load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, 
   int4 w[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) w[c] = p[chunk_index(c, s, r, 3, in.nrhs)];
-  const float nm = in.norm[(size_t)s * in.nrhs + r] * kInvFix * phase;
+  const float nm = in.norm[site_rhs_index(s, r, in.nrhs)] * kInvFix * phase;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     // component k = 3*spin + colour; word k holds (re, im) as (lo, hi)
@@ -386,7 +414,7 @@ QCU_D void load16_block(SpinBlock& v, const CSpinorView& f, int s, int r) {
   int4 w[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) w[c] = p[chunk_index(c, s, r, 3, f.nrhs)];
-  const float2 nm = splat2(f.norm[(size_t)s * f.nrhs + r] * kInvFix);
+  const float2 nm = splat2(f.norm[site_rhs_index(s, r, f.nrhs)] * kInvFix);
 #pragma unroll
   for (int j = 0; j < 6; j++) {
     const int a = word_of(w, j), b = word_of(w, 6 + j);
@@ -417,7 +445,7 @@ QCU_D void store16_block(const SpinorView& f, int s, int r, const SpinBlock& v) 
 #pragma unroll
   for (int c = 0; c < 3; c++)
     p[chunk_index(c, s, r, 3, f.nrhs)] = make_int4(words[4 * c], words[4 * c + 1], words[4 * c + 2], words[4 * c + 3]);
-  f.norm[(size_t)s * f.nrhs + r] = mx;
+  f.norm[site_rhs_index(s, r, f.nrhs)] = mx;
 }
 
 // |v|^2, summed in FP32 pairs (the sloppy solver's dot products)
@@ -436,7 +464,7 @@ QCU_D Cplx<float> block_comp(const SpinBlock& v, int k) {
   return k < 6 ? mk(v.re[k].x, v.im[k].x) : mk(v.re[k - 6].y, v.im[k - 6].y);
 }
 
-template <int PS, int PL, bool DAG, class R>
+template <int PS, int PL, bool DAG, bool ROWS = false, class R>
 QCU_D void hop(Spinor<R>& o, const Geom& g, int parity, int s, int r, const CSpinorView& in,
                const void* gauge, R bc_t) {
 // Paired-FP32 hop for 16-bit spinors (1, default) or the scalar one (0).
@@ -452,10 +480,10 @@ QCU_D void hop(Spinor<R>& o, const Geom& g, int parity, int s, int r, const CSpi
 #pragma unroll
   for (int k = 0; k < 12; k++) o.c[k] = mk(R(0), R(0));
   const Nbrs nb = neighbours(g, s, parity);
-  hop_dir<PS, PL, 0, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<PS, PL, 1, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<PS, PL, 2, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
-  hop_dir<PS, PL, 3, F>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 0, F, ROWS>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 1, F, ROWS>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 2, F, ROWS>(o, g, nb, parity, s, r, in, gauge, bc_t);
+  hop_dir<PS, PL, 3, F, ROWS>(o, g, nb, parity, s, r, in, gauge, bc_t);
 }
 
 }  // namespace qcu

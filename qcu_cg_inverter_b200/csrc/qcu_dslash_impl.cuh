@@ -48,8 +48,26 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_MINB64
 #define QCU_DSLASH_MINB64 1
 #endif
+// RHS-paired kernels (two right-hand sides per thread): blocks of at most
+// 128 threads (half of the 256-slot RHS x site tile); 3 blocks per SM allow
+// 168 registers
+#ifndef QCU_DSLASH_MINB_PAIR
+#define QCU_DSLASH_MINB_PAIR 4
+#endif
+#ifndef QCU_DSLASH_MINB_PAIR_OUT2
+#define QCU_DSLASH_MINB_PAIR_OUT2 QCU_DSLASH_MINB_PAIR
+#endif
+constexpr int dslash_maxt(int op) { return op == OP_HALF_FAST_2 ? 128 : 256; }
+// batched FP64 launches (reliable updates of multi-RHS solves): the
+// 128-register cap with row-at-a-time reconstruction (measured in the 48-RHS
+// 24^3x48 solve: 0.556 vs 0.568 s)
+#ifndef QCU_DSLASH_MINB64_BATCH
+#define QCU_DSLASH_MINB64_BATCH 2
+#endif
 constexpr int dslash_minb(int op, int epi) {
   return op == OP_DOUBLE ? QCU_DSLASH_MINB64
+         : op == OP_DOUBLE_BATCH ? QCU_DSLASH_MINB64_BATCH
+         : op == OP_HALF_FAST_2 ? ((epi & EPI_OUT2) ? QCU_DSLASH_MINB_PAIR_OUT2 : QCU_DSLASH_MINB_PAIR)
          : (op_spinor_prec(op) != PREC_HALF || (op == OP_HALF_FAST_1 && !QCU_DSLASH_CAP_1RHS)) ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
          : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
@@ -78,6 +96,10 @@ QCU_D const void* clover_of(const DslashArgs& a, int r) {
   const int ci = a.clover_idx[r];
   return ci >= 0 ? static_cast<const char*>(a.clover) + a.clover_stride * (size_t)ci : nullptr;
 }
+
+}  // namespace qcu
+#include "qcu_dslash_pair.cuh"
+namespace qcu {
 
 // One output site and RHS of the fast 16-bit operator (16-bit spinors, FP32
 // 18-real links, FP32 block-interleaved clover): the hop and every epilogue in
@@ -135,9 +157,9 @@ QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
   }
 }
 
-// OP selects the storage of spinors, links and clover (OpVariant).
+// One (site, RHS) per thread.
 template <int OP, bool DAG, int EPI, class Fin>
-__global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const DslashArgs a) {
+QCU_D void dslash_site_body(const DslashArgs& a) {
   constexpr int PS = op_spinor_prec(OP), PL = op_link_format(OP), PC = op_clover_prec(OP);
   typedef typename CompReal<PS>::type R;
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
@@ -151,7 +173,7 @@ __global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const
     site_half_fast<DAG, EPI>(a, s, r, nrm);
   } else if (valid) {
     Spinor<R> o;
-    hop<PS, PL, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
+    hop<PS, PL, DAG, OP == OP_DOUBLE_BATCH>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);
     const void* clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) ? clover_of(a, r) : nullptr;
     if (EPI & EPI_CPRE)
       if (clov) clover_apply_site<PC>(o, clov, a.g.Vh_pad, a.parity, s);
@@ -201,12 +223,24 @@ __global__ void __launch_bounds__(256, dslash_minb(OP, EPI)) dslash_kernel(const
   }
 }
 
+// OP selects the storage of spinors, links and clover (OpVariant), and for the
+// fast 16-bit storage the kernel family: OP_HALF_FAST_2 serves two RHS per
+// thread (qcu_dslash_pair.cuh), the others one.
+template <int OP, bool DAG, int EPI, class Fin>
+__global__ void __launch_bounds__(dslash_maxt(OP), dslash_minb(OP, EPI)) dslash_kernel(const DslashArgs a) {
+  if constexpr (OP == OP_HALF_FAST_2)
+    dslash_pair_body<DAG, EPI, Fin>(a);
+  else
+    dslash_site_body<OP, DAG, EPI, Fin>(a);
+}
+
 template <int P, bool DAG>
 static DslashKernelFn pick(int epi, int fin) {
 #define QCU_CASE(E)                                                                     \
   case (E):                                                                             \
     if constexpr (((E)&EPI_CGXR) != 0) {                                                \
-      return fin == FIN_CG_BETA ? dslash_kernel<P, DAG, (E), FinCgBeta> : nullptr;      \
+      if (fin == FIN_CG_BETA) return dslash_kernel<P, DAG, (E), FinCgBeta>;             \
+      return fin == FIN_NONE ? dslash_kernel<P, DAG, (E), FinNone> : nullptr;           \
     } else if constexpr (((E)&EPI_NORM) != 0) {                                         \
       if (fin == FIN_CG_ALPHA) return dslash_kernel<P, DAG, (E), FinCgAlpha>;           \
       return dslash_kernel<P, DAG, (E), FinNone>;                                       \

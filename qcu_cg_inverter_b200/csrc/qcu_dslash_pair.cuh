@@ -1,0 +1,477 @@
+// RHS-paired stencil bodies for batched launches of the fast 16-bit operator
+// (16-bit spinors, FP32 18-real links, FP32 block-interleaved clover).
+//
+// One thread serves one site and two adjacent right-hand sides r, r+1, which
+// occupy the two lanes of paired FP32 instructions (sm_100 FFMA2/FADD2/FMUL2):
+// every component of the spinor is a (lane r, lane r+1) pair for its real and
+// one for its imaginary part. The link, the clover block, the neighbour
+// indices and the addresses are then formed once for two right-hand sides,
+// and every multiply by a link or clover element is one paired instruction
+// for both. Per lane the arithmetic is the same sequence of roundings as the
+// one-RHS-per-thread kernels (spin-paired hop, herm_apply, pack16), so a
+// column's result does not depend on which column shares its thread.
+#pragma once
+#include "qcu_dslash.cuh"
+#include "qcu_kernels.cuh"
+#include "qcu_reduce.cuh"
+
+namespace qcu {
+
+// component k = 3*spin + colour; lane 0 = RHS r, lane 1 = RHS r+1
+struct PairSpinor {
+  float2 re[12], im[12];
+};
+
+// The two RHS lanes of a thread: r0 and r1 = r0 + d (d = 0 when r0 is the
+// last column of an odd batch; lane 1 then repeats lane 0 and is not stored).
+struct RhsPair {
+  int r0, d;
+};
+
+QCU_D int word_k(const int4 w[3], int k) { return word_of(w, k); }
+
+// both lanes' 16-bit chunks of site s: w0 (lane 0) and w1 (lane 1); returns
+// the lanes' norms
+QCU_D float2 load_words_pair(int4 w0[3], int4 w1[3], const CSpinorView& f, int s, RhsPair rp) {
+  const int4* p = static_cast<const int4*>(f.data);
+  const unsigned i0 = (unsigned)chunk_index(0, s, rp.r0, 3, f.nrhs);
+  const unsigned cs = 32u * (unsigned)f.nrhs;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w0[c] = p[i0 + c * cs];
+    w1[c] = p[i0 + c * cs + rp.d];
+  }
+  const unsigned n0 = (unsigned)site_rhs_index(s, rp.r0, f.nrhs);
+  return make_float2(f.norm[n0], f.norm[n0 + rp.d]);
+}
+
+// h = P_mu psi of the neighbour, both lanes, in units of the 16-bit grid, and
+// the scale (norm x phase) the reconstruction applies. Same projector rows as
+// load_project_pair.
+template <int MU, bool FWD, int F>
+QCU_D float2 load_project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], float2 h1im[3], const CSpinorView& in,
+                             int sn, RhsPair rp, float phase) {
+  constexpr int S = FWD ? -F : F;
+  constexpr float fS = (float)S;
+  int4 w0[3], w1[3];
+  const float2 nm = load_words_pair(w0, w1, in, sn, rp);
+  const float2 sc = fmul2(nm, splat2(kInvFix * phase));
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float2 pre[4], pim[4];
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) {
+      const int a = word_k(w0, 3 * sp + c), b = word_k(w1, 3 * sp + c);
+      pre[sp] = dec_lo2(a, b);
+      pim[sp] = dec_hi2(a, b);
+    }
+    if constexpr (MU == 0) {  // h0 = p0 + S i p3, h1 = p1 + S i p2
+      h0re[c] = ffma2(pim[3], splat2(-fS), pre[0]);
+      h0im[c] = ffma2(pre[3], splat2(fS), pim[0]);
+      h1re[c] = ffma2(pim[2], splat2(-fS), pre[1]);
+      h1im[c] = ffma2(pre[2], splat2(fS), pim[1]);
+    } else if constexpr (MU == 1) {  // h0 = p0 - S p3, h1 = p1 + S p2
+      h0re[c] = ffma2(pre[3], splat2(-fS), pre[0]);
+      h0im[c] = ffma2(pim[3], splat2(-fS), pim[0]);
+      h1re[c] = ffma2(pre[2], splat2(fS), pre[1]);
+      h1im[c] = ffma2(pim[2], splat2(fS), pim[1]);
+    } else if constexpr (MU == 2) {  // h0 = p0 + S i p2, h1 = p1 - S i p3
+      h0re[c] = ffma2(pim[2], splat2(-fS), pre[0]);
+      h0im[c] = ffma2(pre[2], splat2(fS), pim[0]);
+      h1re[c] = ffma2(pim[3], splat2(fS), pre[1]);
+      h1im[c] = ffma2(pre[3], splat2(-fS), pim[1]);
+    } else {  // h0 = p0 + S p2, h1 = p1 + S p3
+      h0re[c] = ffma2(pre[2], splat2(fS), pre[0]);
+      h0im[c] = ffma2(pim[2], splat2(fS), pim[0]);
+      h1re[c] = ffma2(pre[3], splat2(fS), pre[1]);
+      h1im[c] = ffma2(pim[3], splat2(fS), pim[1]);
+    }
+  }
+  return sc;
+}
+
+// row i of U h (FWD) or U^dag h for one half-spinor component, both lanes;
+// the order of the multiply-adds is that of su3_row_pair
+template <bool FWD>
+QCU_D void su3_row_rp(float2& re, float2& im, const Link<float>& U, const float2 hre[3], const float2 him[3], int i) {
+  re = make_float2(0.f, 0.f);
+  im = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const Cplx<float> u = FWD ? U.u[i * 3 + j] : U.u[j * 3 + i];
+    const float2 ur = splat2(u.re), ui = splat2(u.im);
+    if (FWD) {
+      re = ffma2(ur, hre[j], re);
+      re = ffma2(fneg2(ui), him[j], re);
+      im = ffma2(ur, him[j], im);
+      im = ffma2(ui, hre[j], im);
+    } else {
+      re = ffma2(ur, hre[j], re);
+      re = ffma2(ui, him[j], re);
+      im = ffma2(ur, him[j], im);
+      im = ffma2(fneg2(ui), hre[j], im);
+    }
+  }
+}
+
+// o += sc * reconstruct(U h): spins 0 and 1 take a = U h0 and b = U h1, spins
+// 2 and 3 the rows of reconstruct() with the sign folded into the scale
+template <int MU, bool FWD, int F>
+QCU_D void mul_reconstruct_rp(PairSpinor& o, const Link<float>& U, const float2 h0re[3], const float2 h0im[3],
+                              const float2 h1re[3], const float2 h1im[3], float2 sc) {
+  constexpr int S = FWD ? -F : F;
+  const float2 sp = fmul2(sc, splat2((float)S)), sn = fmul2(sc, splat2((float)-S));
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    float2 are, aim, bre, bim;
+    su3_row_rp<FWD>(are, aim, U, h0re, h0im, i);
+    su3_row_rp<FWD>(bre, bim, U, h1re, h1im, i);
+    o.re[i] = ffma2(are, sc, o.re[i]);
+    o.im[i] = ffma2(aim, sc, o.im[i]);
+    o.re[3 + i] = ffma2(bre, sc, o.re[3 + i]);
+    o.im[3 + i] = ffma2(bim, sc, o.im[3 + i]);
+    float2 &o2re = o.re[6 + i], &o2im = o.im[6 + i], &o3re = o.re[9 + i], &o3im = o.im[9 + i];
+    if constexpr (MU == 0) {  // o2 -= S i b, o3 -= S i a
+      o2re = ffma2(bim, sp, o2re);
+      o2im = ffma2(bre, sn, o2im);
+      o3re = ffma2(aim, sp, o3re);
+      o3im = ffma2(are, sn, o3im);
+    } else if constexpr (MU == 1) {  // o2 += S b, o3 -= S a
+      o2re = ffma2(bre, sp, o2re);
+      o2im = ffma2(bim, sp, o2im);
+      o3re = ffma2(are, sn, o3re);
+      o3im = ffma2(aim, sn, o3im);
+    } else if constexpr (MU == 2) {  // o2 -= S i a, o3 += S i b
+      o2re = ffma2(aim, sp, o2re);
+      o2im = ffma2(are, sn, o2im);
+      o3re = ffma2(bim, sn, o3re);
+      o3im = ffma2(bre, sp, o3im);
+    } else {  // o2 += S a, o3 += S b
+      o2re = ffma2(are, sp, o2re);
+      o2im = ffma2(aim, sp, o2im);
+      o3re = ffma2(bre, sp, o3re);
+      o3im = ffma2(bim, sp, o3im);
+    }
+  }
+}
+
+template <int MU, int F>
+QCU_D void hop_dir_rp(PairSpinor& o, const Geom& g, const Nbrs& nb, int parity, int s, RhsPair rp,
+                      const CSpinorView& in, const void* gauge, float bc_t) {
+  Link<float> U;
+  float2 h0re[3], h0im[3], h1re[3], h1im[3];
+  LinkIO<LINK_SINGLE18>::load(U, gauge, g.Vh_pad, MU, parity, s);
+  float2 sc = load_project_rp<MU, true, F>(h0re, h0im, h1re, h1im, in, nb.fwd[MU], rp,
+                                           (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
+  mul_reconstruct_rp<MU, true, F>(o, U, h0re, h0im, h1re, h1im, sc);
+  LinkIO<LINK_SINGLE18>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
+  sc = load_project_rp<MU, false, F>(h0re, h0im, h1re, h1im, in, nb.bwd[MU], rp, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
+  mul_reconstruct_rp<MU, false, F>(o, U, h0re, h0im, h1re, h1im, sc);
+}
+
+template <bool DAG>
+QCU_D void hop_rp(PairSpinor& o, const Geom& g, int parity, int s, RhsPair rp, const CSpinorView& in,
+                  const void* gauge, float bc_t) {
+  constexpr int F = DAG ? -1 : 1;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.re[k] = o.im[k] = make_float2(0.f, 0.f);
+  const Nbrs nb = neighbours(g, s, parity);
+  hop_dir_rp<0, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+  hop_dir_rp<1, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+  hop_dir_rp<2, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+  hop_dir_rp<3, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+}
+
+// Element pair of the block-interleaved FP32 clover: chunk q of the lanes'
+// fields holds (b0[2q], b1[2q], b0[2q+1], b1[2q+1]); E = element 2q + h of
+// block b is float b + 2h of the chunk. UNI: both lanes read one field, so the
+// element is one scalar for both lanes.
+template <bool UNI>
+struct CloverPair {
+  const float4* p0;
+  const float4* p1;
+  bool id0, id1;  // lane without a clover term (A = 1)
+  QCU_D float4 chunk0(int q) const { return __ldg(p0 + 32 * q); }
+  // float i of chunk q for each lane (scalar loads straight into the pair),
+  // `id` for a lane without clover
+  QCU_D float2 lanes(int q, int i, float id) const {
+    const float a = __ldg(reinterpret_cast<const float*>(p0 + 32 * q) + i);
+    const float b = __ldg(reinterpret_cast<const float*>(p1 + 32 * q) + i);
+    return make_float2(id0 ? id : a, id1 ? id : b);
+  }
+};
+
+QCU_D float pick4(const float4& w, int i) { return i == 0 ? w.x : (i == 1 ? w.y : (i == 2 ? w.z : w.w)); }
+
+// v <- blockdiag(B0, B1) v for both lanes, block by block; per lane the order
+// of herm_apply
+template <bool UNI>
+QCU_D void clover_apply_rp(PairSpinor& v, const CloverPair<UNI>& C) {
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    float2 ore[6], oim[6];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      float2 d[2];
+      if constexpr (UNI) {
+        const float4 w0 = C.chunk0(q);
+        d[0] = splat2(pick4(w0, b));
+        d[1] = splat2(pick4(w0, b + 2));
+      } else {
+        d[0] = C.lanes(q, b, 1.f);
+        d[1] = C.lanes(q, b + 2, 1.f);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int i = 2 * q + h;
+        ore[i] = fmul2(d[h], v.re[6 * b + i]);
+        oim[i] = fmul2(d[h], v.im[6 * b + i]);
+      }
+    }
+#pragma unroll
+    for (int i = 1; i < 6; i++)
+#pragma unroll
+      for (int j = 0; j < i; j++) {
+        const int k = tri_index(i, j);
+        float2 mre, mim;
+        if constexpr (UNI) {
+          const float4 w0 = C.chunk0(3 + k);
+          mre = splat2(pick4(w0, b));
+          mim = splat2(pick4(w0, b + 2));
+        } else {
+          mre = C.lanes(3 + k, b, 0.f);
+          mim = C.lanes(3 + k, b + 2, 0.f);
+        }
+        const float2 vjr = v.re[6 * b + j], vji = v.im[6 * b + j];
+        const float2 vir = v.re[6 * b + i], vii = v.im[6 * b + i];
+        // o_i += M_ij v_j (cmac), o_j += conj(M_ij) v_i (cmac_conj)
+        ore[i] = ffma2(mre, vjr, ore[i]);
+        ore[i] = ffma2(fneg2(mim), vji, ore[i]);
+        oim[i] = ffma2(mre, vji, oim[i]);
+        oim[i] = ffma2(mim, vjr, oim[i]);
+        ore[j] = ffma2(mre, vir, ore[j]);
+        ore[j] = ffma2(mim, vii, ore[j]);
+        oim[j] = ffma2(mre, vii, oim[j]);
+        oim[j] = ffma2(fneg2(mim), vir, oim[j]);
+      }
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+      v.re[6 * b + i] = ore[i];
+      v.im[6 * b + i] = oim[i];
+    }
+  }
+}
+
+// the lanes' clover fields at site s (parity block `parity`); nullptr = no
+// clover term for that lane
+QCU_D void clover_pair_apply(PairSpinor& v, const void* c0, const void* c1, int Vh_pad, int parity, int s) {
+  if (!c0 && !c1) return;
+  const unsigned i0 = (unsigned)chunk_index(0, s, 0, 18, 1);
+  auto base = [&](const void* c) {
+    return static_cast<const float4*>(c) + (size_t)parity * Vh_pad * 18 + i0;
+  };
+  if (c0 == c1) {
+    CloverPair<true> C{base(c0), base(c0), false, false};
+    clover_apply_rp<true>(v, C);
+  } else {
+    // a lane without clover reads the other lane's field and replaces it by
+    // the identity (A = 1: the same values as skipping the multiply)
+    CloverPair<false> C{base(c0 ? c0 : c1), base(c1 ? c1 : c0), c0 == nullptr, c1 == nullptr};
+    clover_apply_rp<false>(v, C);
+  }
+}
+
+QCU_D void load16_rp(PairSpinor& v, const CSpinorView& f, int s, RhsPair rp) {
+  int4 w0[3], w1[3];
+  const float2 nm = fmul2(load_words_pair(w0, w1, f, s, rp), splat2(kInvFix));
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    const int a = word_k(w0, k), b = word_k(w1, k);
+    v.re[k] = fmul2(dec_lo2(a, b), nm);
+    v.im[k] = fmul2(dec_hi2(a, b), nm);
+  }
+}
+
+// Stores the lanes whose flag is set, with the roundings of pack16(x*sc, ...),
+// one 16-byte chunk of each lane at a time
+QCU_D void store16_rp(const SpinorView& f, int s, RhsPair rp, const PairSpinor& v, bool w0, bool w1) {
+  float m0 = 0.f, m1 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    m0 = fmaxf(m0, fmaxf(fabsf(v.re[k].x), fabsf(v.im[k].x)));
+    m1 = fmaxf(m1, fmaxf(fabsf(v.re[k].y), fabsf(v.im[k].y)));
+  }
+  const float2 sc = make_float2(m0 > 0.f ? kFix / m0 : 0.f, m1 > 0.f ? kFix / m1 : 0.f);
+  int4* p = static_cast<int4*>(f.data);
+  const unsigned i0 = (unsigned)chunk_index(0, s, rp.r0, 3, f.nrhs);
+  const unsigned cs = 32u * (unsigned)f.nrhs;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    int wa[4], wb[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = 4 * c + u;
+      const float2 tre = fadd2(fmul2(v.re[k], sc), splat2(8421376.0f));
+      const float2 tim = fadd2(fmul2(v.im[k], sc), splat2(8421376.0f));
+      wa[u] = (int)__byte_perm(__float_as_uint(tre.x), __float_as_uint(tim.x), 0x5410);
+      wb[u] = (int)__byte_perm(__float_as_uint(tre.y), __float_as_uint(tim.y), 0x5410);
+    }
+    if (w0) p[i0 + c * cs] = make_int4(wa[0], wa[1], wa[2], wa[3]);
+    if (w1) p[i0 + c * cs + rp.d] = make_int4(wb[0], wb[1], wb[2], wb[3]);
+  }
+  const unsigned n0 = (unsigned)site_rhs_index(s, rp.r0, f.nrhs);
+  if (w0) f.norm[n0] = m0;
+  if (w1) f.norm[n0 + rp.d] = m1;
+}
+
+// |v|^2 of each lane in FP32, in the order of site_norm2
+QCU_D float2 norm2_rp(const PairSpinor& v) {
+  float2 n = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    n = ffma2(v.re[k], v.re[k], n);
+    n = ffma2(v.im[k], v.im[k], n);
+  }
+  return n;
+}
+
+// x += alpha p, r -= alpha z for both lanes (FP32 accumulators, 16-bit p),
+// in the order of the one-RHS kernels. The chunks are processed in groups of
+// G (two components each), with every load of a group issued before its
+// stores; the accumulator pointers are declared unaliased so that the next
+// group's loads may also move above this group's stores. Returns |r|^2 of the
+// site per lane (stores only the lanes flagged).
+#ifndef QCU_PAIR_CGXR_GROUP
+#define QCU_PAIR_CGXR_GROUP 3
+#endif
+QCU_D float2 cgxr_pair(const DslashArgs& a, int s, RhsPair rp, const PairSpinor& z, bool w0, bool w1) {
+  constexpr int G = QCU_PAIR_CGXR_GROUP;
+  const int r1 = rp.r0 + rp.d;
+  const float2 al = make_float2((float)a.alpha[rp.r0], (float)a.alpha[r1]);
+  int4 pw0[3], pw1[3];
+  const float2 pn = fmul2(load_words_pair(pw0, pw1, a.pvec, s, rp), splat2(kInvFix));
+  float4* __restrict__ xp = static_cast<float4*>(a.xacc.data);
+  float4* __restrict__ rq = static_cast<float4*>(a.racc.data);
+  const unsigned ix0 = (unsigned)chunk_index(0, s, rp.r0, 6, a.xacc.nrhs);
+  const unsigned ir0 = (unsigned)chunk_index(0, s, rp.r0, 6, a.racc.nrhs);
+  const unsigned xs_ = 32u * (unsigned)a.xacc.nrhs, rs_ = 32u * (unsigned)a.racc.nrhs;
+  float n0 = 0.f, n1 = 0.f;
+#pragma unroll
+  for (int g0 = 0; g0 < 6; g0 += G) {
+    float4 xa[G], xb[G], ra[G], rb[G];
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int q = g0 + u;
+      xa[u] = xp[ix0 + q * xs_];
+      xb[u] = xp[ix0 + q * xs_ + rp.d];
+      ra[u] = rq[ir0 + q * rs_];
+      rb[u] = rq[ir0 + q * rs_ + rp.d];
+    }
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int q = g0 + u;
+      float x0[4] = {xa[u].x, xa[u].y, xa[u].z, xa[u].w}, x1[4] = {xb[u].x, xb[u].y, xb[u].z, xb[u].w};
+      float q0[4] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w}, q1[4] = {rb[u].x, rb[u].y, rb[u].z, rb[u].w};
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int k = 2 * q + h;
+        const float2 p0 = dec16_pair(word_of(pw0, k), pn.x), p1 = dec16_pair(word_of(pw1, k), pn.y);
+        x0[2 * h] += al.x * p0.x;
+        x0[2 * h + 1] += al.x * p0.y;
+        x1[2 * h] += al.y * p1.x;
+        x1[2 * h + 1] += al.y * p1.y;
+        q0[2 * h] -= al.x * z.re[k].x;
+        q0[2 * h + 1] -= al.x * z.im[k].x;
+        q1[2 * h] -= al.y * z.re[k].y;
+        q1[2 * h + 1] -= al.y * z.im[k].y;
+        n0 = fmaf(q0[2 * h], q0[2 * h], n0);
+        n0 = fmaf(q0[2 * h + 1], q0[2 * h + 1], n0);
+        n1 = fmaf(q1[2 * h], q1[2 * h], n1);
+        n1 = fmaf(q1[2 * h + 1], q1[2 * h + 1], n1);
+      }
+      if (w0) {
+        xp[ix0 + q * xs_] = make_float4(x0[0], x0[1], x0[2], x0[3]);
+        rq[ir0 + q * rs_] = make_float4(q0[0], q0[1], q0[2], q0[3]);
+      }
+      if (w1) {
+        xp[ix0 + q * xs_ + rp.d] = make_float4(x1[0], x1[1], x1[2], x1[3]);
+        rq[ir0 + q * rs_ + rp.d] = make_float4(q1[0], q1[1], q1[2], q1[3]);
+      }
+    }
+  }
+  return make_float2(n0, n1);
+}
+
+// o <- x + c o with the 16-bit x decoded component by component
+QCU_D void xpay16_rp(PairSpinor& o, const CSpinorView& f, int s, RhsPair rp, float2 c) {
+  int4 w0[3], w1[3];
+  const float2 nm = fmul2(load_words_pair(w0, w1, f, s, rp), splat2(kInvFix));
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    const int a = word_of(w0, k), b = word_of(w1, k);
+    o.re[k] = ffma2(c, o.re[k], fmul2(dec_lo2(a, b), nm));
+    o.im[k] = ffma2(c, o.im[k], fmul2(dec_hi2(a, b), nm));
+  }
+}
+
+// The kernel body: thread (threadIdx.x, threadIdx.y) serves RHS pair
+// 2*(blockIdx.y*blockDim.x + threadIdx.x) + {0, 1} of site
+// blockIdx.x*blockDim.y + threadIdx.y.
+template <bool DAG, int EPI, class Fin>
+QCU_D void dslash_pair_body(const DslashArgs& a) {
+  const int r0 = 2 * (blockIdx.y * blockDim.x + threadIdx.x);
+  const int s = blockIdx.x * blockDim.y + threadIdx.y;
+  const bool site_ok = s < a.g.Vh;
+  const bool has1 = r0 + 1 < a.nrhs;
+  const bool v0 = site_ok && r0 < a.nrhs && (a.active == nullptr || a.active[r0]);
+  const bool v1 = site_ok && has1 && (a.active == nullptr || a.active[r0 + 1]);
+  const RhsPair rp{r0, has1 ? 1 : 0};
+  double n0 = 0.0, n1 = 0.0;
+  if (v0 || v1) {
+    const int r1 = r0 + rp.d;
+    PairSpinor o;
+    hop_rp<DAG>(o, a.g, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
+    const bool need_clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) != 0;
+    const void* c0 = need_clov ? clover_of(a, r0) : nullptr;
+    const void* c1 = need_clov ? clover_of(a, r1) : nullptr;
+    if (EPI & EPI_CPRE) clover_pair_apply(o, c0, c1, a.g.Vh_pad, a.parity, s);
+    if (EPI & EPI_XPAY) {
+      const float2 c = a.coef ? make_float2((float)a.coef[r0], (float)a.coef[r1]) : splat2((float)a.coef0);
+      if constexpr ((EPI & EPI_CX) != 0) {
+        PairSpinor xv;
+        load16_rp(xv, a.x, s, rp);
+        clover_pair_apply(xv, c0, c1, a.g.Vh_pad, a.parity, s);
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+          o.re[k] = ffma2(c, o.re[k], xv.re[k]);
+          o.im[k] = ffma2(c, o.im[k], xv.im[k]);
+        }
+      } else {
+        xpay16_rp(o, a.x, s, rp, c);
+      }
+      if (EPI & EPI_CPOST) clover_pair_apply(o, c0, c1, a.g.Vh_pad, a.parity, s);
+    }
+    if constexpr ((EPI & EPI_CGXR) != 0) {
+      const float2 n = cgxr_pair(a, s, rp, o, v0, v1);
+      n0 = v0 ? (double)n.x : 0.0;
+      n1 = v1 ? (double)n.y : 0.0;
+    } else {
+      store16_rp(a.out, s, rp, o, v0, v1);
+      if (EPI & EPI_NORM) {
+        const float2 n = norm2_rp(o);
+        n0 = v0 ? (double)n.x : 0.0;
+        n1 = v1 ? (double)n.y : 0.0;
+      }
+    }
+    if (EPI & EPI_OUT2) {
+      clover_pair_apply(o, c0, c1, a.g.Vh_pad, a.parity, s);
+      store16_rp(a.out2, s, rp, o, v0, v1);
+    }
+  }
+  if (EPI & (EPI_NORM | EPI_CGXR)) {
+    double v[2] = {n0, n1};
+    block_reduce_finish<1, Fin, 2>(v, a.nrhs, a.red);
+  }
+}
+
+}  // namespace qcu

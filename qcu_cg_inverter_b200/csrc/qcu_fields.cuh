@@ -107,11 +107,11 @@ template <> struct SpinorIO<PREC_HALF> {
       v.c[4 * c + 2] = mk(lo16(w.z), hi16(w.z));
       v.c[4 * c + 3] = mk(lo16(w.w), hi16(w.w));
     }
-    return f.norm[(size_t)s * f.nrhs + r] * kInvFix;
+    return f.norm[site_rhs_index(s, r, f.nrhs)] * kInvFix;
   }
   static QCU_D void load(Spinor<R>& v, const CSpinorView& f, int s, int r) {
     const int4* p = static_cast<const int4*>(f.data);
-    float nm = f.norm[(size_t)s * f.nrhs + r] * kInvFix;
+    float nm = f.norm[site_rhs_index(s, r, f.nrhs)] * kInvFix;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       int4 w = p[chunk_index(c, s, r, 3, f.nrhs)];
@@ -138,7 +138,7 @@ template <> struct SpinorIO<PREC_HALF> {
       w.w = enc16_pair(v.c[4 * c + 3].re, v.c[4 * c + 3].im, sc);
       p[chunk_index(c, s, r, 3, f.nrhs)] = w;
     }
-    f.norm[(size_t)s * f.nrhs + r] = mx;
+    f.norm[site_rhs_index(s, r, f.nrhs)] = mx;
   }
 };
 

@@ -64,6 +64,9 @@ struct LaunchShape {
 // must be fields of those formats.
 cudaError_t launch_dslash(int op, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape shape,
                           cudaStream_t stream);
+// Test hook: batched launches of the fast 16-bit operator on the RHS-paired
+// kernels for every epilogue (1), on one RHS per thread (0), or as built (-1).
+void set_rhs_pairs_override(int v);
 
 // Number of blocks along x for a field of Vh sites.
 inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }

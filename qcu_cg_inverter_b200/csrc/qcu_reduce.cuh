@@ -25,13 +25,17 @@ struct FinNone {
   static QCU_D void apply(const double*, int, int, void*) {}
 };
 
-constexpr int kMaxWarps = 32;
+// every reducing kernel is launched with at most 256 threads (its
+// __launch_bounds__), so a block has at most 8 warps; the shared array is sized
+// for that (smaller arrays leave more of the SM's memory to the L1 cache)
+constexpr int kMaxWarps = 8;
 
-// vals: NR values of this thread (zero for idle threads). Every thread of the
-// block must call this.
-template <int NR, class Fin>
-QCU_D void block_reduce_finish(double vals[NR], int nrhs, const ReduceArgs& red) {
-  __shared__ double sm[kMaxWarps][NR * 32];
+// vals: NR values for each of the RL right-hand sides of this thread (RHS
+// (blockIdx.y*Rb + threadIdx.x)*RL + j holds vals[j*NR .. j*NR+NR-1]; zero for
+// idle threads). Every thread of the block must call this.
+template <int NR, class Fin, int RL = 1>
+QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs& red) {
+  __shared__ double sm[kMaxWarps][NR * RL * 32];
   __shared__ bool am_last;
   const int Rb = blockDim.x;
   const int tid = threadIdx.y * Rb + threadIdx.x;
@@ -40,18 +44,20 @@ QCU_D void block_reduce_finish(double vals[NR], int nrhs, const ReduceArgs& red)
   const int nwarps = (nthreads + 31) >> 5;
   // reduce over the site lanes of the warp (lanes that share threadIdx.x)
 #pragma unroll
-  for (int k = 0; k < NR; k++)
+  for (int k = 0; k < NR * RL; k++)
     for (int off = 16; off >= Rb; off >>= 1) vals[k] += __shfl_xor_sync(0xffffffffu, vals[k], off);
   if (lane < Rb)
-    for (int k = 0; k < NR; k++) sm[warp][k * 32 + lane] = vals[k];
+    for (int k = 0; k < NR * RL; k++) sm[warp][k * 32 + lane] = vals[k];
   __syncthreads();
   if (threadIdx.y == 0) {
-    int r = blockIdx.y * Rb + threadIdx.x;
-    if (r < nrhs) {
-      for (int k = 0; k < NR; k++) {
-        double acc = 0.0;
-        for (int w = 0; w < nwarps; w++) acc += sm[w][k * 32 + threadIdx.x];
-        red.partial[(size_t)(r * NR + k) * gridDim.x + blockIdx.x] = acc;
+    for (int j = 0; j < RL; j++) {
+      const int r = (blockIdx.y * Rb + threadIdx.x) * RL + j;
+      if (r < nrhs) {
+        for (int k = 0; k < NR; k++) {
+          double acc = 0.0;
+          for (int w = 0; w < nwarps; w++) acc += sm[w][(j * NR + k) * 32 + threadIdx.x];
+          red.partial[(size_t)(r * NR + k) * gridDim.x + blockIdx.x] = acc;
+        }
       }
     }
   }
