@@ -1,5 +1,7 @@
 // Batch engine (qcu_engine.h) and qcuInvert on top of it.
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -276,6 +278,16 @@ int Engine::step(bool* launched) {
   }
   if (lead) QCU_CHECK(replay(o, -1, P.graphs, [&]() -> int { return enqueue_reliable(o, rp_, true); }));
   const int K = chunk_length();
+  static const bool trace = getenv("QCU_TRACE_STEPS") != nullptr;
+  if (trace) {
+    for (int r = 0; r < cap; r++) {
+      if (!owner[r]) continue;
+      fprintf(stderr, "step %lld K %d lead %d | r %d it %d nupd %d ev %d done %d rr %.3e trig %.3e rate %.4f prior %.4f fresh %d\n",
+              (long long)steps, K, (int)lead, r, w.hi(I_ITERS)[r], w.hi(I_NUPD)[r], w.hi(I_EVENT)[r], w.hi(I_DONE)[r],
+              w.hd(D_RR)[r], w.hd(D_TRIG)[r], rate_[r], prior_rate_, (int)fresh_[r]);
+      break;
+    }
+  }
   if (K > 0) {
     QCU_CHECK(run_chunk(o, K, P.graphs));
     // every column that paused during the chunk gets its update now
@@ -321,6 +333,14 @@ int Engine::observe(std::vector<Group*>* retired) {
   for (int r = 0; r < cap; r++) {
     const Group* q = owner[r];
     if (!q || q->state != Group::ITERATING) continue;
+    // a column that finished in this step: its last update stopped without
+    // closing the segment (D_RRPRE is stale), and its rate is no longer
+    // needed; measuring it anyway had left a no-progress rate as the prior of
+    // the next solve's first chunk (a 64-iteration chunk, mostly masked)
+    if (w.hi(I_DONE)[r]) {
+      fresh_[r] = 0;
+      continue;
+    }
     const int it = w.hi(I_ITERS)[r], nupd = w.hi(I_NUPD)[r];
     const double rr = w.hd(D_RR)[r];
     if (fresh_[r]) {
