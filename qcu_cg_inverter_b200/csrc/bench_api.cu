@@ -53,7 +53,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
                                double* bytes) {
   clear_error();
   QCU_CHECK(ctx_check(ctx));
-  if (prec < 0 || prec > 2 || variant < 0 || variant > 2 || nrhs < 1 || iters < 1) {
+  if (prec < 0 || prec > 2 || variant < 0 || variant > 3 || nrhs < 1 || iters < 1) {
     set_error(QCU_ERR_INVALID_ARG, "bad benchmark arguments");
     return QCU_ERR_INVALID_ARG;
   }
@@ -78,8 +78,28 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
     QCU_CHECK_CUDA(launch_spinor_in(prec, g, nrhs, aos.p, (size_t)g.Vh * 12, fx.view(0), st));
     QCU_CHECK_CUDA(cudaStreamSynchronize(st));
   }
+  // variant 3 (the CG update stencil): FP32 (FP64) x and r, a search direction
+  // and per-RHS alpha
+  const int pa = acc_prec(prec);
+  Field fxa, fra, fp;
+  DevBuf alpha;
+  if (variant == 3) {
+    QCU_CHECK(fxa.alloc(pa, g.Vh_pad, nrhs, 1, st));
+    QCU_CHECK(fra.alloc(pa, g.Vh_pad, nrhs, 1, st));
+    QCU_CHECK(fp.alloc(prec, g.Vh_pad, nrhs, 1, st));
+    DevBuf aos;
+    QCU_CHECK(aos.ensure((size_t)g.Vh * 192 * nrhs, st));
+    QCU_CHECK_CUDA(launch_spinor_random((size_t)g.Vh * nrhs, 79, aos.p, st));
+    QCU_CHECK_CUDA(launch_spinor_in(pa, g, nrhs, aos.p, (size_t)g.Vh * 12, fxa.view(0), st));
+    QCU_CHECK_CUDA(launch_spinor_in(pa, g, nrhs, aos.p, (size_t)g.Vh * 12, fra.view(0), st));
+    QCU_CHECK_CUDA(launch_spinor_in(prec, g, nrhs, aos.p, (size_t)g.Vh * 12, fp.view(0), st));
+    std::vector<double> al(nrhs, 1e-3);  // small steps: the fields stay bounded over many launches
+    QCU_CHECK(alpha.ensure(sizeof(double) * nrhs, st));
+    QCU_CHECK_CUDA(cudaMemcpyAsync(alpha.p, al.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+    QCU_CHECK_CUDA(cudaStreamSynchronize(st));
+  }
   int slot = 0;
-  if (variant >= 1) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
+  if (variant == 1 || variant == 2) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
   // the shape the solver would use (tuned when qcuAutotune ran, else the
   // default), unless qcuContextSetShape overrode the single-RHS shape
   LaunchShape sh = (nrhs == 1 && ctx->shape_set) ? ctx->shape1 : ctx_shape(ctx, op, nrhs);
@@ -98,13 +118,23 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   a.coef0 = -0.0169;
   a.bc_t = -1.0;
   a.red = ctx->red.args();
-  int epi = variant == 0 ? 0 : (variant == 1 ? EPI_CPRE : (EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM));
-  for (int k = 0; k < 3; k++) QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
+  if (variant == 3) {
+    a.xacc = fxa.view(0);
+    a.racc = fra.view(0);
+    a.pvec = fp.cview(0);
+    a.alpha = alpha.as<double>();
+  }
+  const int epi = variant == 0   ? 0
+                  : variant == 1 ? EPI_CPRE
+                  : variant == 2 ? (EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM)
+                                 : (EPI_XPAY | EPI_CGXR);
+  const bool dag = variant == 3;  // the CG update stencil applies D^dag
+  for (int k = 0; k < 3; k++) QCU_CHECK_CUDA(launch_dslash(op, dag, epi, FIN_NONE, a, sh, st));
   cudaEvent_t e0, e1;
   QCU_CHECK_CUDA(cudaEventCreate(&e0));
   QCU_CHECK_CUDA(cudaEventCreate(&e1));
   QCU_CHECK_CUDA(cudaEventRecord(e0, st));
-  for (int k = 0; k < iters; k++) QCU_CHECK_CUDA(launch_dslash(op, false, epi, FIN_NONE, a, sh, st));
+  for (int k = 0; k < iters; k++) QCU_CHECK_CUDA(launch_dslash(op, dag, epi, FIN_NONE, a, sh, st));
   QCU_CHECK_CUDA(cudaEventRecord(e1, st));
   QCU_CHECK_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -116,7 +146,8 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   if (bytes) {
     double per_rhs = 8.0 * spinor_b(prec) + spinor_b(prec);
     if (variant == 2) per_rhs += 2.0 * spinor_b(prec);  // xpay input + second output
-    double shared = 8.0 * link_b(op_link_format(op)) + (variant >= 1 ? clov_b(op_clover_prec(op)) : 0.0);
+    if (variant == 3) per_rhs += 2.0 * spinor_b(prec) - spinor_b(prec) + 4.0 * spinor_b(pa);  // x, p in; no out; x, r in and out
+    double shared = 8.0 * link_b(op_link_format(op)) + ((variant == 1 || variant == 2) ? clov_b(op_clover_prec(op)) : 0.0);
     int tiles = (nrhs + sh.Rb - 1) / sh.Rb;
     *bytes = (double)g.Vh * (nrhs * per_rhs + tiles * shared);
   }
@@ -148,7 +179,7 @@ extern "C" int qcuDebugStencil(qcu_context ctx, int prec, int dagger, int epi, i
   cudaStream_t st = ctx->stream;
   const int op = ctx_op(ctx, prec);
   const int ps = op_spinor_prec(op);
-  const int pa = ps == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE;
+  const int pa = acc_prec(ps);
   const size_t per = (size_t)g.Vh * 12;  // complex numbers per AoS spinor
   const size_t aos_bytes = per * 16 * nrhs;
   Field fin, fx, fp, fout, fout2, fxa, fra;

@@ -254,6 +254,7 @@ cudaError_t launch_cg_xr(int pa, int ps, int nsites, int nrhs, SpinorView x, Spi
   if (pa == PREC_DOUBLE && ps == PREC_DOUBLE) QCU_XR(PREC_DOUBLE, PREC_DOUBLE);
   else if (pa == PREC_SINGLE && ps == PREC_SINGLE) QCU_XR(PREC_SINGLE, PREC_SINGLE);
   else if (pa == PREC_SINGLE && ps == PREC_HALF) QCU_XR(PREC_SINGLE, PREC_HALF);
+  else if (pa == PREC_HALF && ps == PREC_HALF) QCU_XR(PREC_HALF, PREC_HALF);
   else return cudaErrorInvalidValue;
 #undef QCU_XR
   return cudaGetLastError();
@@ -266,6 +267,7 @@ cudaError_t launch_cg_p(int pa, int ps, int nsites, int nrhs, SpinorView p, CSpi
   if (pa == PREC_DOUBLE && ps == PREC_DOUBLE) QCU_P(PREC_DOUBLE, PREC_DOUBLE);
   else if (pa == PREC_SINGLE && ps == PREC_SINGLE) QCU_P(PREC_SINGLE, PREC_SINGLE);
   else if (pa == PREC_SINGLE && ps == PREC_HALF) QCU_P(PREC_SINGLE, PREC_HALF);
+  else if (pa == PREC_HALF && ps == PREC_HALF) QCU_P(PREC_HALF, PREC_HALF);
   else return cudaErrorInvalidValue;
 #undef QCU_P
   return cudaGetLastError();
@@ -297,6 +299,7 @@ cudaError_t launch_accumulate(int pl, int nsites, int nrhs, SpinorView xhi, Spin
   dim3 b = blk(sh), g = grd(nsites, nrhs, sh);
   if (pl == PREC_DOUBLE) accumulate_kernel<PREC_DOUBLE><<<g, b, 0, st>>>(nsites, nrhs, xhi, xlo, active);
   else if (pl == PREC_SINGLE) accumulate_kernel<PREC_SINGLE><<<g, b, 0, st>>>(nsites, nrhs, xhi, xlo, active);
+  else if (pl == PREC_HALF) accumulate_kernel<PREC_HALF><<<g, b, 0, st>>>(nsites, nrhs, xhi, xlo, active);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -318,6 +321,7 @@ cudaError_t launch_accumulate_res(int pl, int nsites, int nrhs, SpinorView xhi, 
   dim3 bl = blk(sh), g = grd(nsites, nrhs, sh);
   if (pl == PREC_DOUBLE) accumulate_res_kernel<PREC_DOUBLE><<<g, bl, 0, st>>>(nsites, nrhs, xhi, xlo, b, d, active);
   else if (pl == PREC_SINGLE) accumulate_res_kernel<PREC_SINGLE><<<g, bl, 0, st>>>(nsites, nrhs, xhi, xlo, b, d, active);
+  else if (pl == PREC_HALF) accumulate_res_kernel<PREC_HALF><<<g, bl, 0, st>>>(nsites, nrhs, xhi, xlo, b, d, active);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

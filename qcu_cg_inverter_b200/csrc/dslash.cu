@@ -24,10 +24,10 @@ DslashKernelFn pick_f64b(bool dag, int epi, int fin);
 #ifndef QCU_RHS_PAIRS
 #define QCU_RHS_PAIRS 1
 #endif
-// The CG update stencil (EPI_CGXR: hop, xpay, x and r in FP32) stays on one
-// RHS per thread unless this is 1. Measured in the 48-RHS 24^3x48 solve:
-// 0.519 s with it on one RHS per thread, 0.528 s paired (loads grouped by
-// three chunks), 0.546 s paired with one chunk at a time.
+// The CG update stencil (EPI_CGXR: hop, xpay, x and r update) stays on one
+// RHS per thread unless this is 1. Measured in the 48-RHS 24^3x48 solve with
+// FP32 accumulators: 0.519 s with it on one RHS per thread, 0.528 s paired
+// (loads grouped by three chunks), 0.546 s paired with one chunk at a time.
 #ifndef QCU_PAIR_CGXR
 #define QCU_PAIR_CGXR 0
 #endif

@@ -217,6 +217,20 @@ enum OpVariant : int {
   // cap and row-at-a-time reconstruction)
   OP_DOUBLE_BATCH = 6,
 };
+// Storage of the sloppy solver's accumulators (the partial solution x_lo and
+// the iterated residual r) for a sloppy spinor precision: FP64 for FP64, FP32
+// for FP32, and for 16-bit solves 16-bit like their other spinors (QCU_ACC16
+// 1) or FP32 (0). Measured with 16-bit accumulators: the same iteration and
+// reliable-update counts (16^3x32: 50 and 6; 48-RHS 24^3x48: 47-50), the CG
+// update stencil 666 -> 587 us (24^3x48, 16 RHS), the 48-RHS batch 0.512 ->
+// 0.494 s, config 2 3.50 -> 3.43 ms. The reliable updates bound the error the
+// 16-bit recurrences add.
+#ifndef QCU_ACC16
+#define QCU_ACC16 1
+#endif
+__host__ __device__ constexpr int acc_prec(int ps) {
+  return ps == PREC_DOUBLE ? (int)PREC_DOUBLE : (ps == PREC_HALF && QCU_ACC16) ? (int)PREC_HALF : (int)PREC_SINGLE;
+}
 __host__ __device__ constexpr bool op_fast(int op) {
   return op == OP_HALF_FAST || op == OP_HALF_FAST_1 || op == OP_HALF_FAST_2;
 }

@@ -130,8 +130,8 @@ QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
     // x += alpha p, r -= alpha out (the out of this kernel is the CG's z)
     const float al = (float)a.alpha[r];
     Spinor<float> xv, rv, pv;
-    SpinorIO<PREC_SINGLE>::load(xv, a.xacc, s, r);
-    SpinorIO<PREC_SINGLE>::load(rv, a.racc, s, r);
+    SpinorIO<acc_prec(PREC_HALF)>::load(xv, a.xacc, s, r);
+    SpinorIO<acc_prec(PREC_HALF)>::load(rv, a.racc, s, r);
     SpinorIO<PREC_HALF>::load(pv, a.pvec, s, r);
     float n = 0.f;
 #pragma unroll
@@ -144,8 +144,8 @@ QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
       n = fmaf(rv.c[k].re, rv.c[k].re, n);
       n = fmaf(rv.c[k].im, rv.c[k].im, n);
     }
-    SpinorIO<PREC_SINGLE>::store(a.xacc, s, r, xv);
-    SpinorIO<PREC_SINGLE>::store(a.racc, s, r, rv);
+    SpinorIO<acc_prec(PREC_HALF)>::store(a.xacc, s, r, xv);
+    SpinorIO<acc_prec(PREC_HALF)>::store(a.racc, s, r, rv);
     nrm = n;
   } else {
     store16_block(a.out, s, r, o);
@@ -190,7 +190,7 @@ QCU_D void dslash_site_body(const DslashArgs& a) {
     }
     if constexpr ((EPI & EPI_CGXR) != 0) {
       // x += alpha p, r -= alpha out (the out of this kernel is the CG's z)
-      constexpr int PA = PS == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE;
+      constexpr int PA = acc_prec(PS);
       typedef typename CompReal<PA>::type RA;
       const RA al = (RA)a.alpha[r];
       Spinor<RA> xv, rv;

@@ -335,71 +335,28 @@ QCU_D float2 norm2_rp(const PairSpinor& v) {
   return n;
 }
 
-// x += alpha p, r -= alpha z for both lanes (FP32 accumulators, 16-bit p),
-// in the order of the one-RHS kernels. The chunks are processed in groups of
-// G (two components each), with every load of a group issued before its
-// stores; the accumulator pointers are declared unaliased so that the next
-// group's loads may also move above this group's stores. Returns |r|^2 of the
-// site per lane (stores only the lanes flagged).
-#ifndef QCU_PAIR_CGXR_GROUP
-#define QCU_PAIR_CGXR_GROUP 3
-#endif
-QCU_D float2 cgxr_pair(const DslashArgs& a, int s, RhsPair rp, const PairSpinor& z, bool w0, bool w1) {
-  constexpr int G = QCU_PAIR_CGXR_GROUP;
-  const int r1 = rp.r0 + rp.d;
-  const float2 al = make_float2((float)a.alpha[rp.r0], (float)a.alpha[r1]);
-  int4 pw0[3], pw1[3];
-  const float2 pn = fmul2(load_words_pair(pw0, pw1, a.pvec, s, rp), splat2(kInvFix));
-  float4* __restrict__ xp = static_cast<float4*>(a.xacc.data);
-  float4* __restrict__ rq = static_cast<float4*>(a.racc.data);
-  const unsigned ix0 = (unsigned)chunk_index(0, s, rp.r0, 6, a.xacc.nrhs);
-  const unsigned ir0 = (unsigned)chunk_index(0, s, rp.r0, 6, a.racc.nrhs);
-  const unsigned xs_ = 32u * (unsigned)a.xacc.nrhs, rs_ = 32u * (unsigned)a.racc.nrhs;
-  float n0 = 0.f, n1 = 0.f;
+// x += alpha p, r -= alpha z for one lane, in the order of the one-RHS
+// kernels, accumulators in the storage acc_prec gives (16-bit: x and r are
+// re-encoded with new site norms); returns |r|^2 of the site before storage
+template <int L>
+QCU_D float cgxr_lane(const DslashArgs& a, int s, int r, const PairSpinor& z) {
+  constexpr int PA = acc_prec(PREC_HALF);
+  const float al = (float)a.alpha[r];
+  Spinor<float> xv, rv, pv;
+  SpinorIO<PA>::load(xv, a.xacc, s, r);
+  SpinorIO<PA>::load(rv, a.racc, s, r);
+  SpinorIO<PREC_HALF>::load(pv, a.pvec, s, r);
 #pragma unroll
-  for (int g0 = 0; g0 < 6; g0 += G) {
-    float4 xa[G], xb[G], ra[G], rb[G];
-#pragma unroll
-    for (int u = 0; u < G; u++) {
-      const int q = g0 + u;
-      xa[u] = xp[ix0 + q * xs_];
-      xb[u] = xp[ix0 + q * xs_ + rp.d];
-      ra[u] = rq[ir0 + q * rs_];
-      rb[u] = rq[ir0 + q * rs_ + rp.d];
-    }
-#pragma unroll
-    for (int u = 0; u < G; u++) {
-      const int q = g0 + u;
-      float x0[4] = {xa[u].x, xa[u].y, xa[u].z, xa[u].w}, x1[4] = {xb[u].x, xb[u].y, xb[u].z, xb[u].w};
-      float q0[4] = {ra[u].x, ra[u].y, ra[u].z, ra[u].w}, q1[4] = {rb[u].x, rb[u].y, rb[u].z, rb[u].w};
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int k = 2 * q + h;
-        const float2 p0 = dec16_pair(word_of(pw0, k), pn.x), p1 = dec16_pair(word_of(pw1, k), pn.y);
-        x0[2 * h] += al.x * p0.x;
-        x0[2 * h + 1] += al.x * p0.y;
-        x1[2 * h] += al.y * p1.x;
-        x1[2 * h + 1] += al.y * p1.y;
-        q0[2 * h] -= al.x * z.re[k].x;
-        q0[2 * h + 1] -= al.x * z.im[k].x;
-        q1[2 * h] -= al.y * z.re[k].y;
-        q1[2 * h + 1] -= al.y * z.im[k].y;
-        n0 = fmaf(q0[2 * h], q0[2 * h], n0);
-        n0 = fmaf(q0[2 * h + 1], q0[2 * h + 1], n0);
-        n1 = fmaf(q1[2 * h], q1[2 * h], n1);
-        n1 = fmaf(q1[2 * h + 1], q1[2 * h + 1], n1);
-      }
-      if (w0) {
-        xp[ix0 + q * xs_] = make_float4(x0[0], x0[1], x0[2], x0[3]);
-        rq[ir0 + q * rs_] = make_float4(q0[0], q0[1], q0[2], q0[3]);
-      }
-      if (w1) {
-        xp[ix0 + q * xs_ + rp.d] = make_float4(x1[0], x1[1], x1[2], x1[3]);
-        rq[ir0 + q * rs_ + rp.d] = make_float4(q1[0], q1[1], q1[2], q1[3]);
-      }
-    }
+  for (int k = 0; k < 12; k++) {
+    const float zr = L ? z.re[k].y : z.re[k].x, zi = L ? z.im[k].y : z.im[k].x;
+    xv.c[k].re += al * pv.c[k].re;
+    xv.c[k].im += al * pv.c[k].im;
+    rv.c[k].re -= al * zr;
+    rv.c[k].im -= al * zi;
   }
-  return make_float2(n0, n1);
+  SpinorIO<PA>::store(a.xacc, s, r, xv);
+  SpinorIO<PA>::store(a.racc, s, r, rv);
+  return (float)site_norm2(rv);
 }
 
 // o <- x + c o with the 16-bit x decoded component by component
@@ -452,9 +409,8 @@ QCU_D void dslash_pair_body(const DslashArgs& a) {
       if (EPI & EPI_CPOST) clover_pair_apply(o, c0, c1, a.g.Vh_pad, a.parity, s);
     }
     if constexpr ((EPI & EPI_CGXR) != 0) {
-      const float2 n = cgxr_pair(a, s, rp, o, v0, v1);
-      n0 = v0 ? (double)n.x : 0.0;
-      n1 = v1 ? (double)n.y : 0.0;
+      if (v0) n0 = cgxr_lane<0>(a, s, r0, o);
+      if (v1) n1 = cgxr_lane<1>(a, s, r1, o);
     } else {
       store16_rp(a.out, s, rp, o, v0, v1);
       if (EPI & EPI_NORM) {

@@ -92,7 +92,7 @@ __global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P
 
 int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover) {
   cudaStream_t st = ctx->stream;
-  const int pa = (ps == PREC_DOUBLE) ? PREC_DOUBLE : PREC_SINGLE;
+  const int pa = acc_prec(ps);
   const int vp = ctx->g.Vh_pad;
   if (w.nrhs != nrhs || w.ps != ps || w.op != ctx_op(ctx, ps) || w.vh_pad != vp || w.graph_gen != ctx->clover_gen) w.drop_graphs();
   w.graph_gen = ctx->clover_gen;

@@ -104,13 +104,13 @@ def test_fused_cg_stencil_matches_the_oracle(ctx, oracle, dag):
 
 
 @pytest.mark.parametrize("dag", [0, 1])
-def test_fused_cg_update_matches_between_families_and_fp32(ctx, oracle, dag):
+def test_fused_cg_update_matches_between_families_and_fp64(ctx, oracle, dag):
     """x += alpha p, r -= alpha z with z = x_in + coef D in (the CG's last
-    stencil): bit-identical between the families; against FP64 within FP32
-    accumulator and 16-bit input precision."""
+    stencil): bit-identical between the families; against FP64 on the same
+    quantised inputs within the precision of the accumulators' storage
+    (16-bit with a site norm: 5e-5 of each site's largest component)."""
     c, U, L = ctx
-    inp, xin, p = (quantised(c, oracle, L, spinors(oracle, L, s)) for s in (900, 1000, 1100))
-    xa, ra = spinors(oracle, L, 1200), spinors(oracle, L, 1300)
+    inp, xin, p, xa, ra = (quantised(c, oracle, L, spinors(oracle, L, s)) for s in (900, 1000, 1100, 1200, 1300))
     alpha = [0.5, 0.7, 0.9, 1.1, 1.3]
     res = []
     for pairs in (1, 0):
@@ -127,5 +127,7 @@ def test_fused_cg_update_matches_between_families_and_fp32(ctx, oracle, dag):
         xr = xa[j] + alpha[j] * p[j]
         rr = ra[j] - alpha[j] * z
         for got, ref in ((a["xacc"][j], xr), (a["racc"][j], rr)):
-            assert np.abs(got - ref).max() < 1e-5 * np.abs(ref).max()
-        assert abs(a["norms"][j] - np.vdot(a["racc"][j], a["racc"][j]).real) < 1e-5 * a["norms"][j]
+            err = np.abs(got - ref).max(axis=(1, 2)) / np.abs(ref).max(axis=(1, 2))
+            assert err.max() < 5e-5, (j, err.max())
+        # the norm is of r before it is stored
+        assert abs(a["norms"][j] - np.vdot(rr, rr).real) < 1e-4 * a["norms"][j]
