@@ -88,7 +88,7 @@ int Engine::configure(qcu_context c, int cap_, const EngineParams& p) {
   ctx = c;
   cap = cap_;
   P = p;
-  QCU_CHECK(ws_prepare(ctx, w, cap, P.precision, P.clover));
+  QCU_CHECK(ws_prepare(ctx, w, cap, P.precision, P.clover, P.align));
   const size_t full_b = (size_t)2 * ctx->g.Vh * 12 * 16;
   QCU_CHECK(stage.ensure(full_b * cap, ctx->stream));
   if (!step_ev) QCU_CHECK_CUDA(cudaEventCreateWithFlags(&step_ev, cudaEventDisableTiming));
@@ -280,12 +280,11 @@ int Engine::step(bool* launched) {
   const int K = chunk_length();
   static const bool trace = getenv("QCU_TRACE_STEPS") != nullptr;
   if (trace) {
-    for (int r = 0; r < cap; r++) {
-      if (!owner[r]) continue;
+    for (int r = 0; r < cap; r++) {  // the first column of each group
+      if (!owner[r] || owner[r]->r0 != r) continue;
       fprintf(stderr, "step %lld K %d lead %d | r %d it %d nupd %d ev %d done %d rr %.3e trig %.3e rate %.4f prior %.4f fresh %d\n",
               (long long)steps, K, (int)lead, r, w.hi(I_ITERS)[r], w.hi(I_NUPD)[r], w.hi(I_EVENT)[r], w.hi(I_DONE)[r],
               w.hd(D_RR)[r], w.hd(D_TRIG)[r], rate_[r], prior_rate_, (int)fresh_[r]);
-      break;
     }
   }
   if (K > 0) {

@@ -29,6 +29,11 @@ struct CgDevState {
   int* event;       // set when the RHS paused itself
   int* iters;
   int* breakdown;   // set when pAp <= 0 or not finite
+  int* final_trig;  // 1 when the trigger is the convergence target
+  // when one RHS pauses for its reliable update, every other iterating RHS
+  // whose |r|^2 is within this factor of its own (non-final) trigger pauses
+  // with it, so that their updates coincide (1: off)
+  double align;
 };
 
 struct FinCgAlpha {
@@ -53,6 +58,7 @@ struct FinCgAlpha {
 struct FinCgBeta {
   static QCU_D void apply(const double* res, int nrhs, int NR, void* st) {
     CgDevState* s = static_cast<CgDevState*>(st);
+    bool paused = false;
     for (int r = 0; r < nrhs; r++) {
       if (!s->active[r]) continue;
       double rn = res[r * NR];
@@ -67,6 +73,15 @@ struct FinCgBeta {
       } else if (rn < s->trigger[r]) {
         s->active[r] = 0;
         s->event[r] = 1;
+        paused = true;
+      }
+    }
+    if (paused && s->align > 1.0) {
+      for (int r = 0; r < nrhs; r++) {
+        if (s->active[r] && !s->final_trig[r] && s->rr[r] < s->align * s->trigger[r]) {
+          s->active[r] = 0;
+          s->event[r] = 1;
+        }
       }
     }
   }

@@ -32,6 +32,11 @@ struct EngineParams {
   // most sloppy iterations per step; new RHS join and finished ones leave only
   // between steps, so a server keeps steps short
   int max_chunk = 64;
+  // reliable-update pause alignment (CgDevState::align; 1 = off). Measured:
+  // the 48-RHS 24^3x48 batch 0.495 s off, 0.502 s at 8 (its four kappa groups
+  // then update more often); the serving stream 288 -> 300 RHS solves/s and
+  // p99 2.30 -> 2.00 s at 8
+  double align = 1.0;
 };
 
 // One request: n consecutive columns with one kappa and one clover slot.

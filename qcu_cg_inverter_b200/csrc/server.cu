@@ -168,6 +168,7 @@ int make_resident(qcu_server_s* s, int id) {
     ep.clover = true;
     ep.graphs = true;
     ep.max_chunk = s->P.max_chunk > 0 ? s->P.max_chunk : 8;
+    ep.align = 8.0;
     st = eng->configure(ctx, s->P.columns, ep);
   }
   if (st == QCU_SUCCESS) {

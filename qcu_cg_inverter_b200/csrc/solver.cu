@@ -83,6 +83,7 @@ __global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P
   double q = sqrt(fmax(ar2, 1e-300) / fmax(ne2, 1e-300));
   double target = 0.5 * P.tol * bn / q;
   DV(D_TRIG) = fmax(P.delta2 * ne2, target * target);
+  IV(I_FINAL) = target * target >= P.delta2 * ne2;  // the next pause is the convergence check
   IV(I_ACTIVE) = 1;
   IV(I_EVENT) = 0;
   IV(I_RST) = 1;
@@ -90,7 +91,7 @@ __global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P
 #undef IV
 }
 
-int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover) {
+int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover, double align) {
   cudaStream_t st = ctx->stream;
   const int pa = acc_prec(ps);
   const int vp = ctx->g.Vh_pad;
@@ -127,6 +128,8 @@ int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clove
   w.st.event = w.di(I_EVENT);
   w.st.iters = w.di(I_ITERS);
   w.st.breakdown = w.di(I_BREAK);
+  w.st.final_trig = w.di(I_FINAL);
+  w.st.align = align;
   QCU_CHECK_CUDA(cudaMemcpyAsync(w.dstate.p, &w.st, sizeof(CgDevState), cudaMemcpyHostToDevice, st));
   QCU_CHECK(ctx->red.ensure(ctx->g, nrhs, st, w.shape.Sb));
   return QCU_SUCCESS;
