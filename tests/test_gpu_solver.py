@@ -178,3 +178,23 @@ def test_kernel_launches_are_counted(cuda, qcu_lib):
         n0 = c.launches
         ms, nbytes = c.bench_stencil("half", 1, 1, 5)
         assert c.launches > n0 and ms > 0 and nbytes > 0
+
+
+def test_repeated_solves_reuse_the_first_solves_step_plan(cuda, qcu_lib, oracle):
+    """Successive solves of one context start from the convergence rate the
+    engine measured before. A finished column must not leave a no-progress
+    rate behind: that made every solve after the first open with two
+    64-iteration chunks, mostly masked (2.4x the kernels at delta 1.2e-2)."""
+    L = (8, 8, 8, 8)
+    b = oracle.full_spinor_random(L, 21)
+    with qcu_lib.Context(L) as c:
+        c.generate_gauge(4, 0.4)
+        counts = []
+        for _ in range(3):
+            x = dev(np.zeros_like(b))
+            n0 = c.launches
+            rep = c.invert(x, dev(b), kappa=0.13, csw=1.0, tol=1e-10, precision="half", delta=0.012)[0]
+            assert rep["converged"]
+            counts.append(c.launches - n0)
+        assert counts[1] == counts[2], counts
+        assert counts[1] <= 1.1 * counts[0], counts
