@@ -322,12 +322,16 @@ __global__ void __launch_bounds__(256) clover_apply_kernel(Geom g, int parity, i
   }
 }
 
-// |A r|^2 (reduced per RHS) and u = A^-1 r, FP64, one read of r. Works one
-// chiral block at a time (six components of r, one 6x6 block of A, then of
-// A^-1), so a thread holds one block and half a spinor.
+// |A r|^2 (reduced per RHS) and u = A^-1 r from the FP64 r, one read of r.
+// PU = PREC_DOUBLE: u in FP64, one chiral block at a time (six components of
+// r, one 6x6 block of A, then of A^-1), so a thread holds one block and half a
+// spinor. PU = the sloppy precision: u and r rounded to it (the inputs of the
+// sloppy-operator r_ne), with the roundings of a separate conversion.
+template <int PU>
 __global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, int nrhs, CSpinorView rin, SpinorView u,
-                                                            const void* A, const void* Ainv, size_t clov_stride,
-                                                            const int* clov_idx, const int* active, ReduceArgs red) {
+                                                            SpinorView rs, const void* A, const void* Ainv,
+                                                            size_t clov_stride, const int* clov_idx, const int* active,
+                                                            ReduceArgs red) {
   const int r = blockIdx.y * blockDim.x + threadIdx.x;
   const int s = blockIdx.x * blockDim.y + threadIdx.y;
   const bool valid = (s < g.Vh) && (r < nrhs) && (active == nullptr || active[r]);
@@ -338,8 +342,9 @@ __global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, 
     const int ci = clov_idx ? clov_idx[r] : 0;  // negative slot: A = 1
     const char* a = ci >= 0 ? static_cast<const char*>(A) + clov_stride * (size_t)ci : nullptr;
     const char* ai = ci >= 0 ? static_cast<const char*>(Ainv) + clov_stride * (size_t)ci : nullptr;
-#pragma unroll 1
-    for (int b = 0; b < 2; b++) {
+    typedef typename CompReal<PU>::type RU;
+    Spinor<RU> us, rr;  // sloppy outputs (unused for PU = PREC_DOUBLE)
+    auto block = [&](const int b) {
       Cplx<double> v[6], w[6];
 #pragma unroll
       for (int i = 0; i < 6; i++) {
@@ -357,20 +362,44 @@ __global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, 
       for (int i = 0; i < 6; i++) {
         nrm = fma(v[i].re, v[i].re, nrm);
         nrm = fma(v[i].im, v[i].im, nrm);
-        up[chunk_index(6 * b + i, s, r, 12, u.nrhs)] = make_double2(w[i].re, w[i].im);
+        if constexpr (PU == PREC_DOUBLE) {
+          up[chunk_index(6 * b + i, s, r, 12, u.nrhs)] = make_double2(w[i].re, w[i].im);
+        } else {
+          const double2 x = rp[chunk_index(6 * b + i, s, r, 12, rin.nrhs)];
+          us.c[6 * b + i] = mk((RU)w[i].re, (RU)w[i].im);
+          rr.c[6 * b + i] = mk((RU)x.x, (RU)x.y);
+        }
       }
+    };
+    if constexpr (PU == PREC_DOUBLE) {
+#pragma unroll 1
+      for (int b = 0; b < 2; b++) block(b);
+    } else {  // unrolled, so that the sloppy spinors stay in registers
+      block(0);
+      block(1);
+    }
+    if constexpr (PU != PREC_DOUBLE) {
+      SpinorIO<PU>::store(u, s, r, us);
+      SpinorIO<PU>::store(rs, s, r, rr);
     }
   }
   double vv[1] = {nrm};
   block_reduce_finish<1, FinNone>(vv, nrhs, red);
 }
 
-cudaError_t launch_clover_res(const Geom& g, int parity, int nrhs, CSpinorView r, SpinorView u, const void* A,
-                              const void* Ainv, size_t clov_stride, const int* clov_idx, const int* active,
-                              const ReduceArgs& red, LaunchShape sh, cudaStream_t stream) {
+cudaError_t launch_clover_res(int pu, const Geom& g, int parity, int nrhs, CSpinorView r, SpinorView u, SpinorView rs,
+                              const void* A, const void* Ainv, size_t clov_stride, const int* clov_idx,
+                              const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t stream) {
   dim3 block(sh.Rb, sh.Sb);
   dim3 grid(grid_x(g.Vh, sh.Sb), (nrhs + sh.Rb - 1) / sh.Rb);
-  clover_res_kernel<<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, A, Ainv, clov_stride, clov_idx, active, red);
+#define QCU_CR(P) clover_res_kernel<P><<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, rs, A, Ainv, clov_stride, clov_idx, active, red)
+  switch (pu) {
+    case PREC_DOUBLE: QCU_CR(PREC_DOUBLE); break;
+    case PREC_SINGLE: QCU_CR(PREC_SINGLE); break;
+    case PREC_HALF: QCU_CR(PREC_HALF); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef QCU_CR
   return cudaGetLastError();
 }
 

@@ -236,15 +236,8 @@ int reliable_update(const OpCtx& o) {
     QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? (EPI_CPRE | EPI_XPAY | EPI_NORM) : (EPI_XPAY | EPI_NORM), FIN_NONE,
                   a));
   }
-  if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass
-    QCU_CHECK_CUDA(launch_clover_res(o.ctx->g, 0, w.nrhs, w.y64.cview(0), w.u64.view(0),
-                                     ctx_clover_ptr(o.ctx, PREC_DOUBLE, false), ctx_clover_ptr(o.ctx, PREC_DOUBLE, true),
-                                     ctx_clover_stride(o.ctx, PREC_DOUBLE), w.di(I_CIDX), upd,
-                                     red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
-    o.ctx->launches++;
-  }
   // r_ne = Mhat^dag r only restarts the sloppy recursion (convergence is
-  // decided on the FP64 |A_ee r| above), so with sloppy inner precision it is
+  // decided on the FP64 |A_ee r| below), so with sloppy inner precision it is
   // computed by the sloppy operator from r (and A_ee^-1 r) rounded to the
   // sloppy storage; with FP64 inner precision it stays in FP64
   const bool sloppy_ne = w.ps != PREC_DOUBLE;
@@ -253,14 +246,15 @@ int reliable_update(const OpCtx& o) {
   const Field& uin = sloppy_ne ? w.u : w.u64;
   const Field& tn = sloppy_ne ? w.t : w.t64;
   const Field& zn = sloppy_ne ? w.z : w.z64;
-  if (sloppy_ne) {
+  if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass (and r, u rounded to the sloppy storage)
+    QCU_CHECK_CUDA(launch_clover_res(sloppy_ne ? w.ps : PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0),
+                                     uin.view(0), w.y.view(0), ctx_clover_ptr(o.ctx, PREC_DOUBLE, false),
+                                     ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
+                                     w.di(I_CIDX), upd, red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
+    o.ctx->launches++;
+  } else if (sloppy_ne) {
     QCU_CHECK_CUDA(launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.y.view(0), w.y64.cview(0), upd, nullptr, w.shape, o.st));
     o.ctx->launches++;
-    if (w.clover) {
-      QCU_CHECK_CUDA(
-          launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.u.view(0), w.u64.cview(0), upd, nullptr, w.shape, o.st));
-      o.ctx->launches++;
-    }
   }
   {
     DslashArgs a = op_args(o, pn, 1, w.clover ? uin : rin, tn, upd);
