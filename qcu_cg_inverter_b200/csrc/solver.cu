@@ -245,7 +245,10 @@ int reliable_update(const OpCtx& o) {
   const Field& rin = sloppy_ne ? w.y : w.y64;
   const Field& uin = sloppy_ne ? w.u : w.u64;
   const Field& tn = sloppy_ne ? w.t : w.t64;
-  const Field& zn = sloppy_ne ? w.z : w.z64;
+  // r_ne goes straight into the iterated residual when that has its storage
+  // (the restart then copies nothing; columns that stop are not read again)
+  const bool ne_in_place = (sloppy_ne ? w.ps : PREC_DOUBLE) == w.pa;
+  const Field& zn = ne_in_place ? w.rlo : (sloppy_ne ? w.z : w.z64);
   if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass (and r, u rounded to the sloppy storage)
     QCU_CHECK_CUDA(launch_clover_res(sloppy_ne ? w.ps : PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0),
                                      uin.view(0), w.y.view(0), ctx_clover_ptr(o.ctx, PREC_DOUBLE, false),
@@ -315,10 +318,13 @@ int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select) {
   QCU_CHECK_CUDA(cudaGetLastError());
   const int Vh = o.ctx->g.Vh;
   const bool sloppy_ne = w.ps != PREC_DOUBLE;  // where reliable_update left r_ne
-  QCU_CHECK_CUDA(launch_convert(w.pa, sloppy_ne ? w.ps : PREC_DOUBLE, Vh, nrhs, w.rlo.view(0),
-                                sloppy_ne ? w.z.cview(0) : w.z64.cview(0), w.di(I_RST), nullptr, w.shape, o.st));
+  if ((sloppy_ne ? w.ps : PREC_DOUBLE) != w.pa) {  // else it is in rlo already
+    QCU_CHECK_CUDA(launch_convert(w.pa, sloppy_ne ? w.ps : PREC_DOUBLE, Vh, nrhs, w.rlo.view(0),
+                                  sloppy_ne ? w.z.cview(0) : w.z64.cview(0), w.di(I_RST), nullptr, w.shape, o.st));
+    o.ctx->launches++;
+  }
   QCU_CHECK_CUDA(launch_cg_p(w.pa, w.ps, Vh, nrhs, w.p.view(0), w.rlo.cview(0), w.dd(D_BETA), w.di(I_RST), w.shape, o.st));
-  o.ctx->launches += 3;
+  o.ctx->launches += 2;
   return QCU_SUCCESS;
 }
 
