@@ -268,15 +268,21 @@ int Engine::step(bool* launched) {
     w.graph_gen = ctx->clover_gen;
   }
   const OpCtx o = op();
-  bool lead = !pending.empty();
-  if (!pending.empty()) QCU_CHECK(enqueue_admissions());
-  for (int r = 0; r < cap && !lead; r++) {
+  const bool admitting = !pending.empty();
+  bool others = false;  // iterating columns due for an update
+  for (int r = 0; r < cap && !others; r++) {
     const Group* q = owner[r];
     if (q && q->state == Group::ITERATING && !fresh_[r] && !w.hi(I_DONE)[r] &&
         (w.hi(I_EVENT)[r] || w.hi(I_ITERS)[r] >= P.maxiter))
-      lead = true;
+      others = true;
   }
-  if (lead) QCU_CHECK(replay(o, -1, P.graphs, [&]() -> int { return enqueue_reliable(o, rp_, true); }));
+  if (admitting) QCU_CHECK(enqueue_admissions());
+  if (admitting && !others) {  // only new columns: their residual is bhat
+    QCU_CHECK(replay(o, -2, P.graphs, [&]() -> int { return enqueue_reliable(o, rp_, true, true); }));
+  } else if (admitting || others) {
+    QCU_CHECK(replay(o, -1, P.graphs, [&]() -> int { return enqueue_reliable(o, rp_, true); }));
+  }
+  const bool lead = admitting || others;
   const int K = chunk_length();
   static const bool trace = getenv("QCU_TRACE_STEPS") != nullptr;
   if (trace) {

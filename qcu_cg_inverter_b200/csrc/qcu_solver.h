@@ -77,11 +77,12 @@ DslashArgs op_args(const OpCtx& o, int prec, int parity, const Field& in, const 
 int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& a);
 ReduceArgs red_into(const OpCtx& o, double* result, bool with_state);
 int sloppy_iteration(const OpCtx& o);
-int reliable_update(const OpCtx& o);
+// fresh: every selected column was just admitted (x = 0)
+int reliable_update(const OpCtx& o, bool fresh = false);
 int pull_state(const OpCtx& o);
 int push_state(const OpCtx& o);
 int run_chunk(const OpCtx& o, int K, bool graphs);
-int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select);
+int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select, bool fresh = false);
 
 // Replays (capturing on first use) a CUDA graph of the work `enqueue` puts on
 // the stream; `key` identifies the sequence. The kernels `enqueue` counts

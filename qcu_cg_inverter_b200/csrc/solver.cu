@@ -215,10 +215,15 @@ int sloppy_iteration(const OpCtx& o) {
 // r = bhat - Mhat x_hi, |r|^2 and |A_ee r|^2 (the full-system residual), and
 // r_ne = Mhat^dag r with |r_ne|^2 (into D_RES_R2, D_RES_AR2, D_RES_NE; r_ne
 // lands in z, of the sloppy precision, or z64 for FP64 inner solves).
-int reliable_update(const OpCtx& o) {
+int reliable_update(const OpCtx& o, bool fresh) {
   SolverWorkspace& w = *o.w;
   const int* upd = w.di(I_UPD);
   const int Vh = o.ctx->g.Vh;
+  // Only just-admitted columns (x = 0), clover epilogues and a sloppy inner
+  // solve: r = bhat exactly, so the FP64 operator passes are skipped and the
+  // clover pass reads bhat (the same values as the general path).
+  const bool from_b = fresh && w.clover && w.ps != PREC_DOUBLE;
+  if (!from_b) {
   // x_hi += x_lo and y64 = bhat - x_hi, then r = y64 + kappa^2 A_ee^-1 D_eo
   // A_oo^-1 D_oe x_hi = bhat - Mhat x_hi in place in y64, with |r|^2
   QCU_CHECK_CUDA(launch_accumulate_res(w.pa, Vh, w.nrhs, w.xhi.view(0), w.xlo.view(0), w.bh.cview(0), w.y64.view(0),
@@ -236,6 +241,7 @@ int reliable_update(const OpCtx& o) {
     QCU_CHECK(dsl(o, PREC_DOUBLE, false, w.clover ? (EPI_CPRE | EPI_XPAY | EPI_NORM) : (EPI_XPAY | EPI_NORM), FIN_NONE,
                   a));
   }
+  }
   // r_ne = Mhat^dag r only restarts the sloppy recursion (convergence is
   // decided on the FP64 |A_ee r| below), so with sloppy inner precision it is
   // computed by the sloppy operator from r (and A_ee^-1 r) rounded to the
@@ -250,7 +256,8 @@ int reliable_update(const OpCtx& o) {
   const bool ne_in_place = (sloppy_ne ? w.ps : PREC_DOUBLE) == w.pa;
   const Field& zn = ne_in_place ? w.rlo : (sloppy_ne ? w.z : w.z64);
   if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass (and r, u rounded to the sloppy storage)
-    QCU_CHECK_CUDA(launch_clover_res(sloppy_ne ? w.ps : PREC_DOUBLE, o.ctx->g, 0, w.nrhs, w.y64.cview(0),
+    QCU_CHECK_CUDA(launch_clover_res(sloppy_ne ? w.ps : PREC_DOUBLE, o.ctx->g, 0, w.nrhs,
+                                     from_b ? w.bh.cview(0) : w.y64.cview(0),
                                      uin.view(0), w.y.view(0), ctx_clover_ptr(o.ctx, PREC_DOUBLE, false),
                                      ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
                                      w.di(I_CIDX), upd, red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
@@ -303,7 +310,7 @@ int run_chunk(const OpCtx& o, int K, bool graphs) {
 }
 
 // select + FP64 residual + decide + restart, all on the device
-int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select) {
+int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select, bool fresh) {
   SolverWorkspace& w = *o.w;
   const int nrhs = w.nrhs;
   const int tb = 32, nb = (nrhs + tb - 1) / tb;
@@ -313,7 +320,7 @@ int enqueue_reliable(const OpCtx& o, const RelParams& P, bool select) {
     QCU_CHECK_CUDA(cudaGetLastError());
     o.ctx->launches++;
   }
-  QCU_CHECK(reliable_update(o));
+  QCU_CHECK(reliable_update(o, fresh));
   rel_decide_kernel<<<nb, tb, 0, o.st>>>(nrhs, w.mem.as<double>(), w.di(0), P);
   QCU_CHECK_CUDA(cudaGetLastError());
   const int Vh = o.ctx->g.Vh;
