@@ -237,6 +237,17 @@ long long qcuContextLaunchCount(qcu_context ctx);
 /* The context behind the reference interface (NULL before initGridSize). */
 qcu_context qcuLegacyContext(void);
 
+/* The reference's storage shifts (include/qcu_shift_storage.cuh:14-16,
+ * src/qcu_shift_storage.cu:166-195), also exported under its C++ names
+ * shiftVectorStorage / shiftGaugeStorage. direction 0 (TO_COALESCE): AoS ->
+ * the reference's SoA; 1 (TO_NON_COALESCE): back. Spinor: one parity block,
+ * [V/2][24 doubles] <-> [24][V/2]. Gauge: [4][2][V/2][9 complex] <->
+ * [4][2][12][V/2] (first two rows; going back rebuilds the third as
+ * conj(row0 x row1), where the reference's shift back does nothing). Device
+ * pointers, lattice extents with Lx even; synchronous. */
+int qcuShiftVectorStorage(void* dst, const void* src, int direction, int Lx, int Ly, int Lz, int Lt);
+int qcuShiftGaugeStorage(void* dst, const void* src, int direction, int Lx, int Ly, int Lz, int Lt);
+
 /* Test hook for host-side fault injection: after n more successful device
  * allocations the next one fails as out-of-memory (n < 0 disables). */
 void qcuDebugFailAllocAfter(long long n);

@@ -138,6 +138,41 @@ def full_spinor_random(L, seed: int) -> np.ndarray:
     return spinor_random(2 * Vh, seed).reshape(2, Vh, 4, 3)
 
 
+def shift_vector_storage(src, direction: int) -> np.ndarray:
+    """The reference's spinor storage shift for one parity block
+    (src/qcu_shift_storage.cu:75-118): direction 0 takes the AoS half spinor
+    [site][4][3] complex to the SoA [24][site] doubles (component index
+    2*(spin*3 + colour) + re/im), direction 1 back."""
+    if direction == 0:
+        a = np.ascontiguousarray(src, dtype=np.complex128).reshape(-1, 12)
+        return np.ascontiguousarray(a.view(np.float64).reshape(-1, 24).T)
+    a = np.ascontiguousarray(np.asarray(src, dtype=np.float64).reshape(24, -1).T)
+    return a.view(np.complex128).reshape(-1, 4, 3)
+
+
+def shift_gauge_storage(src, direction: int) -> np.ndarray:
+    """The reference's gauge storage shift (src/qcu_shift_storage.cu:123-161):
+    direction 0 takes [4][2][site][3][3] complex to [4][2][12][site] doubles,
+    the first two rows of each link (index 2*(row*3 + col) + re/im). Direction
+    1 (which the reference leaves undone) goes back and rebuilds the third row
+    as conj(row0 x row1) (src/qcu_clover_dslash.cu:11-16)."""
+    if direction == 0:
+        a = np.ascontiguousarray(src, dtype=np.complex128)
+        nh = a.shape[2]
+        two = a[:, :, :, :2, :].reshape(4, 2, nh, 6)
+        return np.ascontiguousarray(two.view(np.float64).reshape(4, 2, nh, 12).transpose(0, 1, 3, 2))
+    a = np.asarray(src, dtype=np.float64)
+    nh = a.shape[3]
+    two = np.ascontiguousarray(a.transpose(0, 1, 3, 2)).view(np.complex128).reshape(4, 2, nh, 2, 3)
+    U = np.empty((4, 2, nh, 3, 3), np.complex128)
+    U[..., :2, :] = two
+    r0, r1 = two[..., 0, :], two[..., 1, :]
+    U[..., 2, 0] = np.conj(r0[..., 1] * r1[..., 2] - r0[..., 2] * r1[..., 1])
+    U[..., 2, 1] = np.conj(r0[..., 2] * r1[..., 0] - r0[..., 0] * r1[..., 2])
+    U[..., 2, 2] = np.conj(r0[..., 0] * r1[..., 1] - r0[..., 1] * r1[..., 0])
+    return U
+
+
 def dslash(in_half, gauge, L, parity: int, dagger: int = 0, bc_t: float = 1.0) -> np.ndarray:
     out = np.empty_like(in_half)
     lib().orc_dslash(_p(out), _p(np.ascontiguousarray(in_half)), _p(gauge), _L(L), parity, dagger, bc_t)

@@ -128,6 +128,8 @@ def lib():
                               ctypes.POINTER(SolveReport)]),
             "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
             "qcuDebugFailAllocAfter": (None, [ll]),
+            "qcuShiftVectorStorage": (i, [P, P, i, i, i, i, i]),
+            "qcuShiftGaugeStorage": (i, [P, P, i, i, i, i, i]),
             "qcuDebugStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d),
                                     ctypes.POINTER(i), P, P, P, P, P, P, P, ctypes.POINTER(d), i]),
             "qcuAutotune": (i, [P, i, i, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(d)]),
@@ -252,6 +254,18 @@ def MmV_one_round(out, inp, gauge, p, temp):
 
 def preCloverDslash(out, inp, gauge, p, invert_flag=0):
     _check(lib().qcuPreCloverDslash(_ptr(out), _ptr(inp), _ptr(gauge), ctypes.byref(p), int(invert_flag)))
+
+
+def shiftVectorStorage(dst, src, direction: int, lattice) -> None:
+    """reference: src/qcu_shift_storage.cu:166 - one parity block of a spinor,
+    AoS [V/2][24] <-> SoA [24][V/2] (direction 0 = to SoA); device memory."""
+    _check(lib().qcuShiftVectorStorage(_ptr(dst), _ptr(src), int(direction), *[int(v) for v in lattice]))
+
+
+def shiftGaugeStorage(dst, src, direction: int, lattice) -> None:
+    """reference: src/qcu_shift_storage.cu:183 - gauge AoS [4][2][V/2][3][3] <->
+    SoA [4][2][12][V/2] (direction 0 = to SoA; 1 rebuilds the third row)."""
+    _check(lib().qcuShiftGaugeStorage(_ptr(dst), _ptr(src), int(direction), *[int(v) for v in lattice]))
 
 
 def cg_inverter_ref(b_vector, x_vector, gauge, p):

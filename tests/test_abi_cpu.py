@@ -45,7 +45,8 @@ def test_library_exports_reference_cxx_names(qcu_lib):
     syms = exported(qcu_lib.LIB_PATH)
     for m in ("_Z18invertCloverDslashPvS_S_P10QcuParam_si", "_Z15preCloverDslashPvS_S_P10QcuParam_si",
               "_Z20cloverDslashOneRoundPvS_S_P10QcuParam_si", "_Z24fullCloverDslashOneRoundPvS_S_P10QcuParam_si",
-              "_Z27newFullCloverDslashOneRoundPvS_S_P10QcuParam_si", "_Z13MmV_one_roundPvS_S_P10QcuParam_sS_"):
+              "_Z27newFullCloverDslashOneRoundPvS_S_P10QcuParam_si", "_Z13MmV_one_roundPvS_S_P10QcuParam_sS_",
+              "_Z18shiftVectorStoragePvS_iiiii", "_Z17shiftGaugeStoragePvS_iiiii"):
         assert m in syms
 
 

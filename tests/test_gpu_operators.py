@@ -198,3 +198,37 @@ def test_host_pointers_are_staged(cuda, qcu_lib, oracle):
         out = np.zeros_like(x)
         c.dslash(out, x, 1, 0, 1.0)
         assert close(out, oracle.dslash(x, U, L, 1), TOL)
+
+
+@pytest.mark.parametrize("L", LATTICES, ids=lambda L: "x".join(map(str, L)))
+def test_storage_shifts_match_the_oracle(cuda, qcu_lib, oracle, L):
+    """shiftVectorStorage / shiftGaugeStorage (the reference's AoS <-> SoA
+    shifts) against the oracle's restatement: the transposes bit for bit, the
+    rebuilt third row of the links to rounding. The second lattice's half
+    volume (96) is not a multiple of the kernels' 128-site tile."""
+    nh = L[0] * L[1] * L[2] * L[3] // 2
+    psi = oracle.spinor_random(nh, 17)
+    soa = dev(np.zeros(24 * nh))
+    qcu_lib.shiftVectorStorage(soa, dev(psi), 0, L)
+    assert np.array_equal(host(soa, (24, nh)), oracle.shift_vector_storage(psi, 0))
+    back = dev(np.zeros_like(psi))
+    qcu_lib.shiftVectorStorage(back, soa, 1, L)
+    assert np.array_equal(host(back, psi.shape), psi)
+    U = oracle.gauge_random(L, 23, 0.4)
+    g = dev(np.zeros(8 * 12 * nh))
+    qcu_lib.shiftGaugeStorage(g, dev(U), 0, L)
+    ref = oracle.shift_gauge_storage(U, 0)
+    assert np.array_equal(host(g, ref.shape), ref)
+    Ub = dev(np.zeros_like(U))
+    qcu_lib.shiftGaugeStorage(Ub, g, 1, L)
+    got = host(Ub, U.shape)
+    assert np.array_equal(got[..., :2, :], U[..., :2, :])
+    assert close(got, oracle.shift_gauge_storage(ref, 1), 1e-14)
+
+
+def test_storage_shifts_reject_host_pointers(cuda, qcu_lib, oracle):
+    L = (4, 4, 4, 4)
+    psi = oracle.spinor_random(128, 1)
+    with pytest.raises(qcu_lib.QcuError) as e:
+        qcu_lib.shiftVectorStorage(np.zeros(24 * 128), psi, 0, L)
+    assert e.value.code == qcu_lib.QCU_ERR_INVALID_ARG

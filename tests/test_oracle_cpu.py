@@ -139,3 +139,30 @@ def test_reference_cg_flow_on_pure_gauge(oracle):
     C = oracle.clover_build(U, L8, 1.0)
     Ci = oracle.clover_invert(C)
     assert rel(oracle.full_dslash_ref(x, U, C, Ci, L8, 0), b) < 1e-12
+
+
+def test_storage_shift_restatement_follows_the_reference_indexing(oracle):
+    """The oracle's storage shifts against element loops written with the
+    reference's index formulas (src/qcu_shift_storage.cu:75-161): spinor
+    dst[i*nh + s] = src[s*24 + i]; gauge dst[((2*mu+p)*12 + j)*nh + s] =
+    src[((2*mu+p)*nh + s)*18 + j] for the first 12 reals of each link."""
+    import numpy as np
+    L = (4, 2, 2, 2)
+    nh = 16
+    psi = oracle.spinor_random(nh, 3)
+    soa = oracle.shift_vector_storage(psi, 0)
+    flat = psi.reshape(-1).view(np.float64)
+    for s in range(nh):
+        for i in range(24):
+            assert soa[i, s] == flat[s * 24 + i]
+    assert np.array_equal(oracle.shift_vector_storage(soa, 1), psi)
+    U = oracle.gauge_random(L, 5, 0.4)
+    g = oracle.shift_gauge_storage(U, 0)
+    gf = U.reshape(-1).view(np.float64)
+    for mp in range(8):
+        for s in range(nh):
+            for j in range(12):
+                assert g[mp // 2, mp % 2, j, s] == gf[(mp * nh + s) * 18 + j]
+    back = oracle.shift_gauge_storage(g, 1)
+    assert np.array_equal(back[..., :2, :], U[..., :2, :])
+    assert np.abs(back - U).max() < 1e-13  # the rebuilt row of an SU(3) link
