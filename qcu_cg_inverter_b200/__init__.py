@@ -268,6 +268,53 @@ def shiftGaugeStorage(dst, src, direction: int, lattice) -> None:
     _check(lib().qcuShiftGaugeStorage(_ptr(dst), _ptr(src), int(direction), *[int(v) for v in lattice]))
 
 
+def save_fields(path, lattice, gauge=None, spinors=None, **meta) -> None:
+    """Writes fields in the reference's AoS layouts to one .npz file for
+    reproducible fixtures: the lattice extents, an optional gauge field
+    ([4][2][V/2][3][3] complex), optional spinors ([n][2][V/2][4][3] or one
+    [2][V/2][4][3]) and scalar metadata (seed, eps, kappa, ...). Torch tensors
+    are copied to the host."""
+    import numpy as np
+
+    def host(a):
+        if a is None:
+            return None
+        if hasattr(a, "detach"):
+            a = a.detach().cpu().numpy()
+        return np.ascontiguousarray(a, dtype=np.complex128)
+
+    L = np.asarray([int(v) for v in lattice], dtype=np.int64)
+    if L.shape != (4,) or L.min() <= 0 or L[0] % 2:
+        raise ValueError("lattice must be four positive extents with Lx even")
+    vh = int(np.prod(L)) // 2
+    arrays = {"lattice": L}
+    g = host(gauge)
+    if g is not None:
+        if g.size != 4 * 2 * vh * 9:
+            raise ValueError("gauge field does not match the lattice")
+        arrays["gauge"] = g.reshape(4, 2, vh, 3, 3)
+    sp = host(spinors)
+    if sp is not None:
+        if sp.size % (2 * vh * 12):
+            raise ValueError("spinors do not match the lattice")
+        arrays["spinors"] = sp.reshape(-1, 2, vh, 4, 3)
+    for k, v in meta.items():
+        arrays["meta_" + k] = np.asarray(v)
+    np.savez_compressed(path, **arrays)
+
+
+def load_fields(path):
+    """Reads a file written by save_fields: (lattice, gauge or None, spinors or
+    None, metadata dict)."""
+    import numpy as np
+    with np.load(path) as f:
+        lattice = tuple(int(v) for v in f["lattice"])
+        gauge = f["gauge"] if "gauge" in f else None
+        spinors = f["spinors"] if "spinors" in f else None
+        meta = {k[5:]: f[k][()] for k in f.files if k.startswith("meta_")}
+    return lattice, gauge, spinors, meta
+
+
 def cg_inverter_ref(b_vector, x_vector, gauge, p):
     """The reference CG flow with (iterations, converged) returned."""
     it, conv = ctypes.c_int(0), ctypes.c_int(0)

@@ -92,3 +92,17 @@ def test_server_entry_points_are_declared(qcu_lib):
     for n in ("qcuServerCreate", "qcuServerSubmit", "qcuServerPoll", "qcuServerQuery", "qcuServerRunTrace",
               "qcuServerDestroy", "qcuHostAlloc"):
         assert n in names
+
+
+def test_field_dumps_round_trip(qcu_lib, oracle, tmp_path):
+    import numpy as np
+    L = (4, 4, 2, 2)
+    U = oracle.gauge_random(L, 9, 0.3)
+    psi = np.stack([oracle.full_spinor_random(L, 40 + r) for r in range(3)])
+    f = tmp_path / "fields.npz"
+    qcu_lib.save_fields(f, L, gauge=U, spinors=psi, seed=9, eps=0.3)
+    L2, U2, psi2, meta = qcu_lib.load_fields(f)
+    assert L2 == L and np.array_equal(U2, U) and np.array_equal(psi2, psi)
+    assert meta == {"seed": 9, "eps": 0.3}
+    with pytest.raises(ValueError):
+        qcu_lib.save_fields(f, L, gauge=U[:, :, :1])
