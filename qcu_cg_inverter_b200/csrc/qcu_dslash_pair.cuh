@@ -28,8 +28,6 @@ struct RhsPair {
   int r0, d;
 };
 
-QCU_D int word_k(const int4 w[3], int k) { return word_of(w, k); }
-
 // both lanes' 16-bit chunks of site s: w0 (lane 0) and w1 (lane 1); returns
 // the lanes' norms
 QCU_D float2 load_words_pair(int4 w0[3], int4 w1[3], const CSpinorView& f, int s, RhsPair rp) {
@@ -61,7 +59,7 @@ QCU_D float2 load_project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], flo
     float2 pre[4], pim[4];
 #pragma unroll
     for (int sp = 0; sp < 4; sp++) {
-      const int a = word_k(w0, 3 * sp + c), b = word_k(w1, 3 * sp + c);
+      const int a = word_of(w0, 3 * sp + c), b = word_of(w1, 3 * sp + c);
       pre[sp] = dec_lo2(a, b);
       pim[sp] = dec_hi2(a, b);
     }
@@ -286,7 +284,7 @@ QCU_D void load16_rp(PairSpinor& v, const CSpinorView& f, int s, RhsPair rp) {
   const float2 nm = fmul2(load_words_pair(w0, w1, f, s, rp), splat2(kInvFix));
 #pragma unroll
   for (int k = 0; k < 12; k++) {
-    const int a = word_k(w0, k), b = word_k(w1, k);
+    const int a = word_of(w0, k), b = word_of(w1, k);
     v.re[k] = fmul2(dec_lo2(a, b), nm);
     v.im[k] = fmul2(dec_hi2(a, b), nm);
   }
