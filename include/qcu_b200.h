@@ -259,7 +259,8 @@ void qcuDebugFailAllocAfter(long long n);
  * output). csw_eff[r] <= 0 means no clover term for RHS r. out, out2, xacc
  * and racc are read before and written after the launch; norms[r] receives
  * the launch's per-RHS sums. rhs_pairs: 1 = RHS-paired kernels, 0 = one RHS
- * per thread, -1 = as built. */
+ * per thread, -1 = as built; the choice is process-wide for the duration of
+ * the call, so this hook must not run concurrently with other solves. */
 int qcuDebugStencil(qcu_context ctx, int precision, int dagger, int epi, int nrhs, const double* csw_eff,
                     const double* coef, const double* alpha, const int* active, const void* in, const void* x,
                     const void* pvec, void* out, void* out2, void* xacc, void* racc, double* norms,
