@@ -134,11 +134,15 @@ int qcuDslash(qcu_context ctx, void* out, const void* in, int parity, int dagger
  * pool, or a loop that cannot take cudaMalloc's implicit synchronisation).
  * No counterpart in the reference. Instead of the staging fields qcuDslash
  * allocates on first use, it uses a fixed 6 MiB scratch array compiled into
- * the library (held on every GPU that loads it), so the lattice's half volume
- * may be at most 16384 sites (larger: QCU_ERR_INVALID_ARG). in/out must be
- * device pointers. Calls that overlap on the GPU share that array and race.
- * The first call on a device looks up the array's device address; make that
- * first call before starting any stream capture. */
+ * the library, so the lattice's half volume may be at most 16384 sites
+ * (larger: QCU_ERR_INVALID_ARG). in/out must be device memory of the
+ * context's GPU. Calls that overlap on the GPU share that array and race.
+ * qcuContextCreate does the per-device set-up (the array's device address,
+ * the code of the kernels the call launches), so the 6 MiB are held from the
+ * first context on a device until the process exits; if that set-up failed
+ * there, the first call retries it, so make one call before any stream
+ * capture. The address is cached per device: after a cudaDeviceReset the
+ * library must not be used again in that process. */
 int qcuDslashNoAlloc(qcu_context ctx, void* out, const void* in, int parity, int dagger, double bc_t);
 /* out = A in (inverse = 0) or A^-1 in (inverse = 1), full spinors, with
  * A = 1 + csw_eff*T (csw_eff = kappa*c_sw; 1 reproduces the reference). */

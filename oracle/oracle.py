@@ -20,6 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_LIB_PATH = os.path.join(HERE, "_ref", "libqcu_ref.so")
+# the reference's sources (its cg_inverter/ directory), needed only to build
+# _ref/libqcu_ref.so; by default a checkout beside this repository
+REF_SRC_DIR = os.environ.get("QCU_REFERENCE_DIR",
+                             os.path.join(os.path.dirname(HERE), "..", "reference", "cg_inverter"))
 
 _lib = None
 
@@ -28,9 +32,9 @@ def build(ref: bool = False) -> None:
     """Compile the oracle (and, if asked and the reference sources exist, the
     reference library) with oracle/Makefile."""
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/cg_inverter"):
+    if ref and os.path.isdir(REF_SRC_DIR):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={os.path.abspath(REF_SRC_DIR)}"] + targets, check=True)
 
 
 def lib():
@@ -62,6 +66,8 @@ def lib():
             "orc_cg_inverter_ref": (i, [P, P, P, I4, i, ctypes.POINTER(ctypes.c_int)]),
             "orc_apply_full": (None, [P, P, P, P, I4, d, d, i]),
             "orc_solve_schur": (i, [P, P, P, I4, d, d, d, d, i, ctypes.POINTER(ctypes.c_double)]),
+            "orc_solve_schur_cl": (i, [P, P, P, P, P, I4, d, d, d, i, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_int)]),
             "orc_schur_apply": (None, [P, P, P, P, I4, d, d, i]),
             "orc_num_threads": (i, []),
             "orc_set_num_threads": (None, [i]),
@@ -254,6 +260,17 @@ def solve_schur(b, gauge, L, kappa, csw, bc_t=-1.0, tol=1e-10, maxiter=100000):
     res = ctypes.c_double(0)
     it = lib().orc_solve_schur(_p(x), _p(b), _p(gauge), _L(L), kappa, csw, bc_t, tol, maxiter, ctypes.byref(res))
     return x, it, res.value
+
+
+def solve_schur_cl(b, gauge, clover, cinv, L, kappa, bc_t=-1.0, tol=1e-10, maxiter=100000):
+    """solve_schur with a prebuilt clover A (clover_build at kappa*c_sw) and its
+    inverse; returns (x, iterations, true residual, true-residual checks)."""
+    x = np.empty_like(b)
+    res = ctypes.c_double(0)
+    chk = ctypes.c_int(0)
+    it = lib().orc_solve_schur_cl(_p(x), _p(b), _p(gauge), _p(clover), _p(cinv), _L(L), kappa, bc_t, tol, maxiter,
+                                  ctypes.byref(res), ctypes.byref(chk))
+    return x, it, res.value, chk.value
 
 
 def set_threads(n: int) -> None:

@@ -689,50 +689,72 @@ static double norm2_real(const double* x, size_t n) {
   return d[0];
 }
 
-int orc_solve_schur(double* x, const double* b, const double* gauge, const int L[4], double kappa,
-                    double csw, double bc_t, double tol, int maxiter, double* true_res) {
+/* CG on Mhat^dag Mhat x_e = Mhat^dag bhat with a prebuilt clover A and its
+ * inverse, stopping on the true residual of the full system, |b - M x|/|b| <
+ * tol. The full residual is measured at checks only: at x = 0, and whenever
+ * the iterated normal-equation residual |r|^2 falls below the level at which
+ * the true residual is predicted at tol/2, the prediction using the ratio
+ * q = |b - M x| / |Mhat^dag (bhat - Mhat x_e)| of the last check (the
+ * convergence trigger of the B200 library's FP64 solve, so both stop by the
+ * same rule). After a failed check the recursion restarts from the
+ * recomputed residual, keeping the search direction with
+ * beta = |r_new|^2 / |r_old|^2. The CG iteration itself is the plain CGNR
+ * recursion of the reference's cg (src/cg_inverter.cu:181-256) on the
+ * Hermitian normal operator. */
+int orc_solve_schur_cl(double* x, const double* b, const double* gauge, const double* clover,
+                       const double* cinv, const int L[4], double kappa, double bc_t, double tol,
+                       int maxiter, double* true_res, int* checks) {
   geom_t g = geom(L);
   size_t nh = g.Vh * 12, n = g.V * 12;
-  double* clover = (double*)malloc(sizeof(double) * 144 * g.V);
-  double* cinv = (double*)malloc(sizeof(double) * 144 * g.V);
-  orc_clover_build(clover, gauge, L, kappa * csw);
-  orc_clover_invert(cinv, clover, g.V);
   double* bh = (double*)malloc(sizeof(double) * 2 * nh);
   double* t = (double*)malloc(sizeof(double) * 2 * nh);
   double* r = (double*)malloc(sizeof(double) * 2 * nh);
   double* p = (double*)malloc(sizeof(double) * 2 * nh);
   double* y = (double*)malloc(sizeof(double) * 2 * nh);
   double* z = (double*)malloc(sizeof(double) * 2 * nh);
-  double* rhs = (double*)malloc(sizeof(double) * 2 * nh);
   double* full = (double*)malloc(sizeof(double) * 2 * n);
   const double* be = b;
   const double* bo = b + nh * 2;
+  const double kk[2] = {kappa, 0};
   /* bhat = A_ee^-1 (b_e + kappa D_eo A_oo^-1 b_o) */
   memcpy(t, bo, sizeof(double) * 2 * nh);
   orc_clover_apply(t, cinv + g.Vh * 144, g.Vh);
   orc_dslash(bh, t, gauge, L, 0, 0, bc_t);
   memcpy(t, be, sizeof(double) * 2 * nh);
-  const double kk[2] = {kappa, 0};
   orc_caxpy(t, bh, kk, nh);
   memcpy(bh, t, sizeof(double) * 2 * nh);
   orc_clover_apply(bh, cinv, g.Vh);
-  orc_schur_apply(rhs, bh, gauge, cinv, L, kappa, bc_t, 1);
-  double rhs2 = norm2_real(rhs, nh);
   double b2 = norm2_real(b, n);
   memset(x, 0, sizeof(double) * 2 * n);
   double* xe = x;
   double* xo = x + 2 * nh;
-  int iters = 0;
-  double tol_ne = tol * 1e-2;
-  double res = 1.0;
-  for (int attempt = 0; attempt < 6; attempt++) {
-    /* r = rhs - Mhat^dag Mhat x */
+  int iters = 0, nchk = 0;
+  double res = 1.0, rr = 0.0;
+  memset(p, 0, sizeof(double) * 2 * nh);
+  for (;;) {
+    /* check: x_o = A_oo^-1 (b_o + kappa D_oe x_e), then |b - M x| */
+    orc_dslash(t, xe, gauge, L, 1, 0, bc_t);
+    memcpy(xo, bo, sizeof(double) * 2 * nh);
+    orc_caxpy(xo, t, kk, nh);
+    orc_clover_apply(xo, cinv + g.Vh * 144, g.Vh);
+    orc_apply_full(full, x, gauge, clover, L, kappa, bc_t, 0);
+    for (size_t i = 0; i < 2 * n; i++) full[i] = b[i] - full[i];
+    const double ar2 = norm2_real(full, n);
+    res = b2 > 0 ? sqrt(ar2 / b2) : 0.0;
+    nchk++;
+    if (res < tol || iters >= maxiter || !isfinite(res)) break;
+    /* r = Mhat^dag (bhat - Mhat x_e) */
     orc_schur_apply(y, xe, gauge, cinv, L, kappa, bc_t, 0);
-    orc_schur_apply(z, y, gauge, cinv, L, kappa, bc_t, 1);
-    for (size_t i = 0; i < 2 * nh; i++) r[i] = rhs[i] - z[i];
-    memcpy(p, r, sizeof(double) * 2 * nh);
-    double rr = norm2_real(r, nh);
-    while (rr > tol_ne * tol_ne * rhs2 && iters < maxiter) {
+    for (size_t i = 0; i < 2 * nh; i++) y[i] = bh[i] - y[i];
+    orc_schur_apply(r, y, gauge, cinv, L, kappa, bc_t, 1);
+    const double ne2 = norm2_real(r, nh);
+    const double beta = rr > 0 ? ne2 / rr : 0.0;
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < 2 * nh; i++) p[i] = r[i] + beta * p[i];
+    rr = ne2;
+    const double q = sqrt(fmax(ar2, 1e-300) / fmax(ne2, 1e-300));
+    const double target = 0.5 * tol * sqrt(b2) / q;
+    while (rr > target * target && iters < maxiter) {
       orc_schur_apply(y, p, gauge, cinv, L, kappa, bc_t, 0);
       double pap = norm2_real(y, nh);
       orc_schur_apply(z, y, gauge, cinv, L, kappa, bc_t, 1);
@@ -741,26 +763,29 @@ int orc_solve_schur(double* x, const double* b, const double* gauge, const int L
       orc_caxpy(xe, p, pa, nh);
       orc_caxpy(r, z, ma, nh);
       double rr_new = norm2_real(r, nh);
-      double beta = rr_new / rr;
+      double bt = rr_new / rr;
       rr = rr_new;
 #pragma omp parallel for schedule(static)
-      for (size_t i = 0; i < 2 * nh; i++) p[i] = r[i] + beta * p[i];
+      for (size_t i = 0; i < 2 * nh; i++) p[i] = r[i] + bt * p[i];
       iters++;
     }
-    /* x_o = A_oo^-1 (b_o + kappa D_oe x_e) */
-    orc_dslash(t, xe, gauge, L, 1, 0, bc_t);
-    memcpy(xo, bo, sizeof(double) * 2 * nh);
-    orc_caxpy(xo, t, kk, nh);
-    orc_clover_apply(xo, cinv + g.Vh * 144, g.Vh);
-    orc_apply_full(full, x, gauge, clover, L, kappa, bc_t, 0);
-    for (size_t i = 0; i < 2 * n; i++) full[i] = b[i] - full[i];
-    res = sqrt(norm2_real(full, n) / b2);
-    if (res < tol || iters >= maxiter) break;
-    tol_ne *= 0.1;
   }
   if (true_res) *true_res = res;
-  free(clover); free(cinv); free(bh); free(t); free(r); free(p); free(y); free(z); free(rhs); free(full);
+  if (checks) *checks = nchk;
+  free(bh); free(t); free(r); free(p); free(y); free(z); free(full);
   return iters;
+}
+
+int orc_solve_schur(double* x, const double* b, const double* gauge, const int L[4], double kappa,
+                    double csw, double bc_t, double tol, int maxiter, double* true_res) {
+  geom_t g = geom(L);
+  double* clover = (double*)malloc(sizeof(double) * 144 * g.V);
+  double* cinv = (double*)malloc(sizeof(double) * 144 * g.V);
+  orc_clover_build(clover, gauge, L, kappa * csw);
+  orc_clover_invert(cinv, clover, g.V);
+  int it = orc_solve_schur_cl(x, b, gauge, clover, cinv, L, kappa, bc_t, tol, maxiter, true_res, NULL);
+  free(clover); free(cinv);
+  return it;
 }
 
 int orc_num_threads(void) {

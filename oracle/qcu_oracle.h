@@ -72,10 +72,17 @@ int orc_cg_inverter_ref(double* x, const double* b, const double* gauge, const i
 void orc_apply_full(double* out, const double* in, const double* gauge, const double* clover,
                     const int L[4], double kappa, double bc_t, int dagger);
 /* Even-odd Schur CGNR on Mhat^dag Mhat, Mhat = 1 - kappa^2 A_ee^-1 D_eo A_oo^-1 D_oe,
- * odd sites reconstructed. Stops when the true full residual |b-Mx|/|b| < tol.
+ * odd sites reconstructed. Stops when the true full residual |b-Mx|/|b| < tol, checked
+ * where the iterated residual predicts it (see orc_solve_schur_cl).
  * Returns iterations; *true_res receives the final true relative residual. */
 int orc_solve_schur(double* x, const double* b, const double* gauge, const int L[4], double kappa,
                     double csw, double bc_t, double tol, int maxiter, double* true_res);
+/* The same with a prebuilt clover A (clover) and its inverse (clover_inv), so
+ * that the setup is timed apart from the solve; *checks (may be NULL) receives
+ * the number of true-residual checks. */
+int orc_solve_schur_cl(double* x, const double* b, const double* gauge, const double* clover,
+                       const double* clover_inv, const int L[4], double kappa, double bc_t, double tol,
+                       int maxiter, double* true_res, int* checks);
 /* The Schur operator and its adjoint on even half spinors (for operator tests). */
 void orc_schur_apply(double* out, const double* in, const double* gauge, const double* clover_inv,
                      const int L[4], double kappa, double bc_t, int dagger);

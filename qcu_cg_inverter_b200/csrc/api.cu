@@ -140,6 +140,16 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+bool is_device_ptr_on(const void* p, int device) {
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == device);
+}
+
 // ---------------------------------------------------------------------------
 // context helpers
 // ---------------------------------------------------------------------------
@@ -485,6 +495,9 @@ int qcuContextCreate(qcu_context* out, const int lattice[4], int device) {
     delete ctx;
     return st;
   }
+  // qcuDslashNoAlloc's device set-up happens here, so that its calls take no
+  // device memory; a failure is reported by that entry point, not here
+  if (noalloc_prepare(device) != QCU_SUCCESS) clear_error();
   *out = ctx;
   return QCU_SUCCESS;
 }

@@ -120,6 +120,16 @@ cudaError_t launch_spinor_out(int prec, const Geom& g, int count, CSpinorView sr
   return cudaGetLastError();
 }
 
+// Loads the code of the FP64 spinor conversion kernels on the current device
+// (with lazy module loading a kernel's module is otherwise loaded, and its
+// device memory taken, at its first launch).
+cudaError_t preload_spinor_io_f64() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, spinor_in_kernel<PREC_DOUBLE>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, spinor_out_kernel<PREC_DOUBLE>);
+  return e;
+}
+
 // ---------------------------------------------------------------------------
 // seeded synthetic fields (same streams and arithmetic as the CPU oracle)
 // ---------------------------------------------------------------------------

@@ -20,11 +20,21 @@
 // at zero). Calls whose work overlaps on the GPU - from two host threads, or
 // two contexts on different streams of the same device - race on the array.
 //
-// The device address of the array is looked up once per device with
-// cudaGetSymbolAddress during the first call made on that device (with that
-// device current); host code must never hand the array's host-side name to a
-// kernel. That first call should come before any stream capture the caller
-// starts.
+// Set-up, once per device and with that device current: the device address of
+// the array is looked up with cudaGetSymbolAddress, and the code of the
+// kernels the entry point launches is loaded (under lazy module loading a
+// module, the array's included, is loaded and its device memory taken at
+// first use). qcuContextCreate runs this set-up, so the 6 MiB are taken when
+// the first context is created on a device and a call takes no device memory
+// at all. Should that set-up fail there, the first call retries it (and then
+// it may load code), so a context that is to be used under stream capture
+// should make one call first. Host code must never hand the array's host-side
+// name to a kernel.
+//
+// The address is cached per device for the life of the process: after a
+// cudaDeviceReset (or a reset of the primary context) every context of this
+// library is invalid anyway, and neither it nor this entry point may be used
+// again in that process.
 #include <string.h>
 
 #include <mutex>
@@ -43,7 +53,10 @@ static __device__ __align__(256) double2 g_noalloc_scratch[2 * kNoAllocMaxVh * 1
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
 
-static int noalloc_scratch(int device, double2** out) {
+typedef void (*DslashKernelFn)(const DslashArgs);
+DslashKernelFn pick_f64(bool dag, int epi, int fin);
+
+static int noalloc_lookup(int device) {
   if (device < 0 || device >= kNoAllocMaxDevices) {
     set_error(QCU_ERR_UNSUPPORTED, "device index beyond the no-alloc scratch table");
     return QCU_ERR_UNSUPPORTED;
@@ -53,8 +66,24 @@ static int noalloc_scratch(int device, double2** out) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // device `device` is current
     if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    // the kernels of a call: AoS -> internal, the FP64 hop (D and D^dag),
+    // internal -> AoS
+    e = preload_spinor_io_f64();
+    cudaFuncAttributes fa;
+    for (int dag = 0; dag < 2 && e == cudaSuccess; dag++) {
+      DslashKernelFn fn = pick_f64(dag != 0, 0, FIN_NONE);
+      e = fn ? cudaFuncGetAttributes(&fa, fn) : cudaErrorInvalidDeviceFunction;
+    }
+    if (e != cudaSuccess) return cuda_status(e, "loading the no-alloc kernels");
     g_noalloc_addr[device] = p;
   }
+  return QCU_SUCCESS;
+}
+
+int noalloc_prepare(int device) { return noalloc_lookup(device); }
+
+static int noalloc_scratch(int device, double2** out) {
+  QCU_CHECK(noalloc_lookup(device));
   *out = static_cast<double2*>(g_noalloc_addr[device]);
   return QCU_SUCCESS;
 }
@@ -76,8 +105,9 @@ extern "C" int qcuDslashNoAlloc(qcu_context ctx, void* out, const void* in, int 
     set_error(QCU_ERR_INVALID_ARG, "bad dslash arguments");
     return QCU_ERR_INVALID_ARG;
   }
-  if (!is_device_ptr(out) || !is_device_ptr(in)) {
-    set_error(QCU_ERR_INVALID_ARG, "qcuDslashNoAlloc takes device pointers only (host data would need staging)");
+  if (!is_device_ptr_on(out, ctx->device) || !is_device_ptr_on(in, ctx->device)) {
+    set_error(QCU_ERR_INVALID_ARG,
+              "qcuDslashNoAlloc takes device pointers of the context's GPU only (host data would need staging)");
     return QCU_ERR_INVALID_ARG;
   }
   if (!ctx->gauge_loaded) {

@@ -166,6 +166,12 @@ int ctx_autotune(qcu_context ctx, int prec, int nrhs, double* best_ms);
 
 // staging of user pointers that may live on the host
 bool is_device_ptr(const void* p);
+// device memory of `device` (or managed memory)
+bool is_device_ptr_on(const void* p, int device);
+// qcuDslashNoAlloc's set-up on the current device (noalloc.cu): the scratch
+// array's device address and the code of the kernels it launches
+int noalloc_prepare(int device);
+cudaError_t preload_spinor_io_f64();
 
 // kernel launchers (defined in the .cu files)
 cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, void* d18,
