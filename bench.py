@@ -54,10 +54,15 @@ LATTICE = (16, 16, 16, 32)
 KAPPA, CSW, EPS, BC_T, TOL = 0.1375, 1.0, 0.4, -1.0, 1e-10
 GAUGE_SEED, SOURCE_SEED = 20241, 7
 ROOF_LATTICE = (32, 32, 32, 64)
-# DRAM bytes (read + write) per output site of the fused 16-bit stencil,
-# from an ncu capture of one launch at 32^4 (592.9 MB for 524288 sites);
-# the traffic grows with the number of sites, so a 32^3x64 launch moves twice that
-ROOF_TRAFFIC_BYTES_PER_SITE = 592.9e6 / 524288
+# DRAM bytes (read + write) per output site of the fused 16-bit stencil, per
+# storage of links and clover, from ncu captures of one launch (the traffic
+# grows with the number of sites): FP32 links and clover at 32^4 (592.9 MB for
+# 524288 sites)
+ROOF_TRAFFIC_BYTES_PER_SITE = {"fast": 592.9e6 / 524288, "compact": None}
+# storage behind the 16-bit solves (qcuContextSetHalfOperator) and its description
+STORAGE = {"auto": None, "fast": True, "compact": False}
+DTYPE = {"fast": "f32 arithmetic; 16-bit spinors, FP32 links (18 reals) and FP32 clover; f64 reliable updates",
+         "compact": "f32 arithmetic; 16-bit spinors, 16-bit 12-real links and 16-bit clover; f64 reliable updates"}
 METRIC = "CG time to |r|/|b|<1e-10, mixed vs FP64 (16^3x32 Wilson-clover, kappa 0.1375, c_sw 1)"
 
 
@@ -275,6 +280,7 @@ def run_large(roof, torch, device, flush, args):
 
     out = {"workload": "32^3x64 Wilson-clover CG to true residual 1e-10", "lattice": ROOF_LATTICE,
            "kappa": LARGE_KAPPA, "csw": CSW, "eps": LARGE_EPS, "bc_t": "antiperiodic",
+           "dtype": DTYPE[roof.half_storage(1)],
            "l2": "256 MB buffer written between timed steps (fields exceed L2)"}
     res = {}
     for prec, steps in ((args.precision, 3), ("double", 2)):
@@ -320,6 +326,7 @@ def run_ours(args, world, rank, local):
     device = torch.device("cuda", local)
     ctx = q.Context(LATTICE, local)
     ctx.generate_gauge(GAUGE_SEED, EPS)
+    ctx.set_half_operator(STORAGE[args.storage])
     V = ctx.volume
     b = torch.empty(V * 12, dtype=torch.complex128, device=device)
     ctx.generate_spinor(b, 1, SOURCE_SEED + rank)
@@ -371,12 +378,15 @@ def run_ours(args, world, rank, local):
         roof = q.Context(ROOF_LATTICE, local)
         V_roof = roof.volume
         roof.generate_gauge(GAUGE_SEED, LARGE_EPS)
+        roof.set_half_operator(STORAGE[args.storage])
         for p in ("half", "double"):
             roof.autotune(p, 1)
         ms, nbytes = roof.bench_stencil("half", 2, 1, 50)
         ms_hop64, bytes_hop64 = roof.bench_stencil("double", 0, 1, 20)
         ms_hop16, bytes_hop16 = roof.bench_stencil("half", 0, 1, 50)
         achieved = nbytes / (ms / 1e3) / 1e9
+        roof_storage = roof.half_storage(1)
+        tps = ROOF_TRAFFIC_BYTES_PER_SITE[roof_storage]
         # in-solve kernels at the headline size (fields L2-resident)
         ms_small, nbytes_small = ctx.bench_stencil("half", 2, 1, 50)
         ms_hop64_small, _ = ctx.bench_stencil("double", 0, 1, 20)
@@ -387,7 +397,7 @@ def run_ours(args, world, rank, local):
             "metric": METRIC, "value": world * steps / t_mixed, "unit": "solves/s", "n_gpus": world,
             "steps": steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 arithmetic; 16-bit spinors, FP32 links (18 reals) and FP32 clover; f64 reliable updates",
+            "dtype": DTYPE[ctx.half_storage(1)],
             "data": "synthetic (seeded SU(3) links exp(0.4iH), seeded Gaussian source)",
             "config": {"workload": "16^3x32 Wilson-clover even-odd CG to true residual 1e-10", "lattice": LATTICE,
                        "kappa": KAPPA, "csw": CSW, "bc_t": "antiperiodic", "precision": args.precision,
@@ -402,10 +412,10 @@ def run_ours(args, world, rank, local):
                     "d2h_bytes_per_step": V * 12 * 16},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": src,
-                         "traffic": ROOF_TRAFFIC_BYTES_PER_SITE * (V_roof // 2),
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
-                                           "32^4, scaled by the site count",
-                         "kernel": "dslash half hop+A^-1+xpay+out2+norm, 32^3x64, 1 RHS",
+                         "traffic": tps * (V_roof // 2) if tps else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                           "per site, times the sites of this launch",
+                         "kernel": "dslash half hop+A^-1+xpay+out2+norm, 32^3x64, 1 RHS", "storage": DTYPE[roof_storage],
                          "bytes_per_launch": nbytes, "ms_per_launch": ms},
             "dslash": {"lattice": ROOF_LATTICE,
                        "fp64_hop_GBps": bytes_hop64 / (ms_hop64 / 1e3) / 1e9, "fp64_hop_ms": ms_hop64,
@@ -756,6 +766,7 @@ def run_stencil(args):
     hbm, src = peaks()
     with q.Context(tuple(args.stencil), 0) as c:
         c.generate_gauge(GAUGE_SEED, 0.5)
+        c.set_half_operator(STORAGE[args.storage])
         if args.sb:
             c.set_shape(1, args.sb)
         elif not args.no_autotune:  # else: the shape from QCU_TUNE_CACHE or the default
@@ -763,6 +774,7 @@ def run_stencil(args):
         ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
     gbs = nbytes / (ms / 1e3) / 1e9
     print(json.dumps({"stencil": args.stencil, "precision": args.precision, "variant": args.variant,
+                      "storage": c.half_storage(args.nrhs),
                       "nrhs": args.nrhs, "ms_per_launch": ms, "bytes_per_launch": nbytes, "GBps": gbs,
                       "frac": gbs / hbm, "peak_source": src}), flush=True)
 
@@ -776,6 +788,9 @@ def main():
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--sb", type=int, default=0, help="site lanes per block for --stencil (0 = library default)")
     ap.add_argument("--no-autotune", action="store_true", help="--stencil: keep the cached or default shape")
+    ap.add_argument("--storage", default="auto", choices=sorted(STORAGE),
+                    help="links and clover behind --precision half: 16-bit (compact), FP32 (fast), or the "
+                         "library's choice by lattice size and RHS count (auto)")
     ap.add_argument("--multi", action="store_true", help="the 48-RHS 24^3x48 batch against FP64 single-RHS")
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)

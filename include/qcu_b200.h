@@ -109,10 +109,18 @@ void* qcuContextGetStream(qcu_context ctx);
 /* Thread-block shape (RHS lanes x site lanes, 32..256 threads) of the
  * context's single-RHS kernels; the autotuner sets it from measurements. */
 int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes);
-/* Storage behind QCU_PREC_HALF: fast_links = 1 (default) keeps 16-bit spinors
- * with FP32 links (all 18 reals, nothing to decode or rebuild) and an FP32
- * clover inverse; 0 keeps links and clover in 16-bit too (smallest footprint). */
+/* Storage behind QCU_PREC_HALF: fast_links = 1 keeps 16-bit spinors with FP32
+ * links (all 18 reals, nothing to decode or rebuild) and an FP32 clover
+ * inverse; 0 keeps links (12 reals) and the clover inverse in 16-bit too
+ * (about half the bytes per site); -1 (the default) picks per solve: 16-bit
+ * links and clover for single-RHS solves on half volumes of 131072 sites or
+ * more (where the fields exceed L2 and bytes bound the stencil), FP32 links
+ * and clover otherwise (batched solves, whose link and clover loads serve
+ * every RHS, and small lattices). */
 int qcuContextSetHalfOperator(qcu_context ctx, int fast_links);
+/* The storage a 16-bit solve of nrhs right-hand sides would use on this
+ * context: 1 = FP32 links and clover, 0 = 16-bit (negative: an error code). */
+int qcuContextHalfOperator(qcu_context ctx, int nrhs);
 /* Device bytes the context holds now. */
 long long qcuContextDeviceBytes(qcu_context ctx);
 

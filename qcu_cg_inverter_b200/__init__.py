@@ -114,6 +114,7 @@ def lib():
             "qcuContextGetStream": (P, [P]),
             "qcuContextSetShape": (i, [P, i, i]),
             "qcuContextSetHalfOperator": (i, [P, i]),
+            "qcuContextHalfOperator": (i, [P, i]),
             "qcuContextDeviceBytes": (ll, [P]),
             "qcuContextLaunchCount": (ll, [P]),
             "qcuLoadGauge": (i, [P, P]),
@@ -432,9 +433,18 @@ class Context:
         """Thread-block shape (RHS lanes x site lanes) of single-RHS kernels."""
         _check(lib().qcuContextSetShape(self._h, int(rhs_lanes), int(site_lanes)))
 
-    def set_half_operator(self, fast_links: bool):
-        """16-bit solver storage: FP32 links/clover (True, default) or 16-bit (False)."""
-        _check(lib().qcuContextSetHalfOperator(self._h, int(bool(fast_links))))
+    def set_half_operator(self, fast_links):
+        """16-bit solver storage: FP32 links/clover (True), 16-bit (False), or
+        chosen per solve by lattice size and RHS count (None, the default)."""
+        _check(lib().qcuContextSetHalfOperator(self._h, -1 if fast_links is None else int(bool(fast_links))))
+
+    def half_storage(self, nrhs: int = 1) -> str:
+        """'fast' (FP32 links and clover) or 'compact' (16-bit): what a 16-bit
+        solve of nrhs right-hand sides uses on this context."""
+        v = lib().qcuContextHalfOperator(self._h, int(nrhs))
+        if v < 0:
+            _check(-v)
+        return "fast" if v == 1 else "compact"
 
     def autotune(self, precision, nrhs: int = 1):
         """Times every launch shape for (precision, nrhs); returns (Rb, Sb, ms)."""

@@ -546,8 +546,18 @@ int qcuContextSetShape(qcu_context ctx, int rhs_lanes, int site_lanes) {
 int qcuContextSetHalfOperator(qcu_context ctx, int fast_links) {
   clear_error();
   QCU_CHECK(ctx_check(ctx));
-  ctx->half_op = fast_links ? OP_HALF_FAST : OP_HALF;
+  ctx->half_op = fast_links < 0 ? -1 : (fast_links ? OP_HALF_FAST : OP_HALF);
   return QCU_SUCCESS;
+}
+
+int qcuContextHalfOperator(qcu_context ctx, int nrhs) {
+  clear_error();
+  QCU_CHECK(ctx_check(ctx));
+  if (nrhs < 1) {
+    set_error(QCU_ERR_INVALID_ARG, "nrhs must be positive");
+    return QCU_ERR_INVALID_ARG;
+  }
+  return ctx_op(ctx, PREC_HALF, nrhs) == OP_HALF ? 0 : 1;
 }
 
 long long qcuContextDeviceBytes(qcu_context ctx) {

@@ -63,7 +63,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   }
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
-  const int op = ctx_op(ctx, prec);  // the operator variant the solver uses for this precision
+  const int op = ctx_op(ctx, prec, nrhs);  // the operator variant the solver uses for this precision
   Field fin, fout, fx, fout2;
   QCU_CHECK(fin.alloc(prec, g.Vh_pad, nrhs, 1, st));
   QCU_CHECK(fout.alloc(prec, g.Vh_pad, nrhs, 1, st));
@@ -177,7 +177,7 @@ extern "C" int qcuDebugStencil(qcu_context ctx, int prec, int dagger, int epi, i
   }
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
-  const int op = ctx_op(ctx, prec);
+  const int op = ctx_op(ctx, prec, nrhs);
   const int ps = op_spinor_prec(op);
   const int pa = acc_prec(ps);
   const size_t per = (size_t)g.Vh * 12;  // complex numbers per AoS spinor

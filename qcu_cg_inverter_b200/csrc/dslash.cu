@@ -12,6 +12,7 @@ DslashKernelFn pick_f16x(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x1(bool dag, int epi, int fin);
 DslashKernelFn pick_f16p(bool dag, int epi, int fin);
 DslashKernelFn pick_f64b(bool dag, int epi, int fin);
+DslashKernelFn pick_f16c1(bool dag, int epi, int fin);
 
 // Batched FP64 launches on their own kernel family (OP_DOUBLE_BATCH: capped,
 // row-at-a-time reconstruction) (1) or on the single-RHS one (0).
@@ -32,6 +33,13 @@ DslashKernelFn pick_f64b(bool dag, int epi, int fin);
 #define QCU_PAIR_CGXR 0
 #endif
 
+// Single-RHS launches of the compact 16-bit operator (OP_HALF) on their own
+// kernel family (OP_HALF_1: paired decode, block-paired epilogues) (1) or on
+// the generic one (0).
+#ifndef QCU_COMPACT_1RHS
+#define QCU_COMPACT_1RHS 1
+#endif
+
 static int g_pairs_override = -1;
 void set_rhs_pairs_override(int v) { g_pairs_override = v; }
 
@@ -46,7 +54,7 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
   switch (prec) {
     case PREC_DOUBLE: fn = (QCU_F64_BATCH && a.nrhs > 1) ? pick_f64b(dagger, epi, fin) : pick_f64(dagger, epi, fin); break;
     case PREC_SINGLE: fn = pick_f32(dagger, epi, fin); break;
-    case PREC_HALF: fn = pick_f16(dagger, epi, fin); break;
+    case PREC_HALF: fn = (a.nrhs == 1 && QCU_COMPACT_1RHS) ? pick_f16c1(dagger, epi, fin) : pick_f16(dagger, epi, fin); break;
     case OP_HALF_FAST:
       if (a.nrhs == 1) {
         fn = pick_f16x1(dagger, epi, fin);

@@ -484,7 +484,7 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
       if (std::find(distinct.begin(), distinct.end(), k * P.csw) == distinct.end()) distinct.push_back(k * P.csw);
     QCU_CHECK(ctx_clover_reserve(ctx, (int)distinct.size()));
   }
-  if (P.autotune && !ctx_is_tuned(ctx, ctx_op(ctx, P.precision), nrhs))
+  if (P.autotune && !ctx_is_tuned(ctx, ctx_op(ctx, P.precision, nrhs), nrhs))
     QCU_CHECK(ctx_autotune(ctx, P.precision, nrhs, nullptr));
   if (!ctx->engine) ctx->engine = new Engine();
   Engine& E = *ctx->engine;

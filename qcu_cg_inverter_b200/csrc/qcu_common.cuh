@@ -198,7 +198,10 @@ enum Prec : int { PREC_DOUBLE = 0, PREC_SINGLE = 1, PREC_HALF = 2 };
 // Link storage formats (LinkIO): the three above keep 12 reals (two rows) and
 // rebuild the third row; LINK_SINGLE18 keeps all 18 reals in FP32 (80 bytes
 // with padding), so a kernel does no decoding and no reconstruction.
-enum LinkFormat : int { LINK_SINGLE18 = 3 };
+// LINK_HALF_RAW is the 16-bit 12-real storage of PREC_HALF read by the
+// single-RHS compact kernels: entries stay in units of the 16-bit grid
+// (x 32767) and the stencil folds the 1/32767 into its per-neighbour scale.
+enum LinkFormat : int { LINK_SINGLE18 = 3, LINK_HALF_RAW = 4 };
 
 // Operator variants (the `prec` argument of launch_dslash): spinor, link and
 // clover storage of one stencil instantiation.
@@ -216,6 +219,9 @@ enum OpVariant : int {
   // the storage of OP_DOUBLE; the kernels of its batched launches (a register
   // cap and row-at-a-time reconstruction)
   OP_DOUBLE_BATCH = 6,
+  // the storage of OP_HALF (everything 16-bit); the kernels its single-RHS
+  // launches use (paired decode, block-paired epilogues)
+  OP_HALF_1 = 7,
 };
 // Storage of the sloppy solver's accumulators (the partial solution x_lo and
 // the iterated residual r) for a sloppy spinor precision: FP64 for FP64, FP32
@@ -234,7 +240,9 @@ __host__ __device__ constexpr int acc_prec(int ps) {
 __host__ __device__ constexpr bool op_fast(int op) {
   return op == OP_HALF_FAST || op == OP_HALF_FAST_1 || op == OP_HALF_FAST_2;
 }
-__host__ __device__ constexpr int op_base(int op) { return op == OP_DOUBLE_BATCH ? (int)OP_DOUBLE : op; }
+__host__ __device__ constexpr int op_base(int op) {
+  return op == OP_DOUBLE_BATCH ? (int)OP_DOUBLE : op == OP_HALF_1 ? (int)OP_HALF : op;
+}
 __host__ __device__ constexpr int op_spinor_prec(int op) { return op_fast(op) ? (int)PREC_HALF : op_base(op); }
 __host__ __device__ constexpr int op_link_format(int op) { return op_fast(op) ? (int)LINK_SINGLE18 : op_base(op); }
 __host__ __device__ constexpr int op_clover_prec(int op) { return op_fast(op) ? (int)PREC_SINGLE : op_base(op); }

@@ -120,7 +120,9 @@ struct qcu_context_s {
   // resident gauge field (internal layout): 12-real double/single/16-bit and
   // 18-real single (the fast 16-bit operator's links)
   qcu::DevBuf gauge64, gauge32, gauge16, gauge18;
-  int half_op = qcu::OP_HALF_FAST;  // operator variant behind QCU_PREC_HALF
+  // operator variant behind QCU_PREC_HALF: OP_HALF_FAST, OP_HALF, or -1 =
+  // chosen per solve (ctx_op)
+  int half_op = -1;
   bool gauge_loaded = false;
   long long gauge_version = 0;
   const void* legacy_gauge_src = nullptr;  // AoS pointer last ingested by the legacy API
@@ -157,7 +159,19 @@ const void* ctx_clover_ptr(qcu_context ctx, int op, bool inverse);
 size_t ctx_clover_stride(qcu_context ctx, int op);
 const void* ctx_gauge(qcu_context ctx, int op);
 // the operator variant that serves spinor precision `prec`
-inline int ctx_op(qcu_context ctx, int prec) { return prec == PREC_HALF ? ctx->half_op : prec; }
+// Half volumes from which single-RHS 16-bit solves keep links and clover in
+// 16-bit (OP_HALF) by default. Measured on B200: at 32^3x64 (fields far beyond
+// L2) the fused CG stencil takes 162 instead of 208 us and the solve 28.8
+// instead of 35.8 ms; at 16^3x32 (the FP32 fields, 80 MB, fit in L2) the FP32
+// links are faster per launch (14.4 vs 16.4 us) and the solves are even.
+constexpr int kCompactMinVh = 131072;
+// the operator variant that serves spinor precision `prec` for a solve or
+// launch of nrhs right-hand sides
+inline int ctx_op(qcu_context ctx, int prec, int nrhs) {
+  if (prec != PREC_HALF) return prec;
+  if (ctx->half_op >= 0) return ctx->half_op;
+  return (nrhs == 1 && ctx->g.Vh_pad >= kCompactMinVh) ? (int)OP_HALF : (int)OP_HALF_FAST;
+}
 
 // launch shapes (tune.cu)
 LaunchShape ctx_shape(qcu_context ctx, int prec, int nrhs);

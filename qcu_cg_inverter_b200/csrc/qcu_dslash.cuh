@@ -203,6 +203,30 @@ QCU_D int word_of(const int4 w[3], int k) {
   return l == 0 ? c.x : (l == 1 ? c.y : (l == 2 ? c.z : c.w));
 }
 
+// 16-bit 12-real links in units of the 16-bit grid: rows 0 and 1 decoded two
+// entries per paired subtraction, row 2 = conj(row0 x row1) / 32767 in the
+// same units (the stencil scales the product by 1/32767 per neighbour).
+template <> struct LinkIO<LINK_HALF_RAW> {
+  typedef float R;
+  static QCU_D void load(Link<R>& L, const void* gauge, int Vh_pad, int mu, int parity, int s) {
+    const int2* p = static_cast<const int2*>(gauge) + (size_t)(mu * 2 + parity) * Vh_pad * 3;
+    int2 w[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) w[c] = __ldg(p + chunk_index(c, s, 0, 3, 1));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2 re = dec_lo2(w[c].x, w[c].y), im = dec_hi2(w[c].x, w[c].y);
+      L.u[2 * c] = mk(re.x, im.x);
+      L.u[2 * c + 1] = mk(re.y, im.y);
+    }
+    su3_reconstruct(L);
+#pragma unroll
+    for (int k = 6; k < 9; k++) L.u[k] = kInvFix * L.u[k];
+  }
+};
+// the factor that converts a link of format PL to its value
+template <int PL> QCU_HD constexpr float link_unit() { return PL == LINK_HALF_RAW ? kInvFix : 1.f; }
+
 // h = P_mu psi of the 16-bit neighbour spinor, spin-paired, in units of its
 // 16-bit grid; returns the scale (norm times `phase`) that the reconstruction
 // applies (the hop is linear, so scaling U h equals scaling h). Same projector
@@ -305,11 +329,12 @@ QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, 
                         const void* gauge, float bc_t) {
   Link<float> U;
   HalfPair h;
+  constexpr float unit = link_unit<PL>();
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : 1.f);
+  float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t * unit : unit);
   mul_reconstruct_pair<MU, true, F>(o, U, h, sc);
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : 1.f);
+  sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t * unit : unit);
   mul_reconstruct_pair<MU, false, F>(o, U, h, sc);
 }
 
@@ -406,6 +431,49 @@ QCU_D void clover_apply_block(SpinBlock& v, const void* clov, int Vh_pad, int pa
   for (int j = 0; j < 6; j++) {
     v.re[j] = ore[j];
     v.im[j] = oim[j];
+  }
+}
+
+// v <- blockdiag(B0, B1) v, 16-bit clover (CloverIO<PREC_HALF>: per site 36
+// words, block b's element word k at word 18b + k, and one norm): the words of
+// the two blocks decode into the lanes of one pair, so the multiply is the
+// one of clover_apply_block; the site's scale (norm / 32767) is applied to
+// the result.
+QCU_D void clover_apply_block16(SpinBlock& v, const void* clov, int Vh_pad, int parity, int s) {
+  const int4* p = static_cast<const int4*>(clov) + (size_t)parity * Vh_pad * 9;
+  int4 c[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) c[q] = __ldg(p + chunk_index(q, s, 0, 9, 1));
+  const float nm = __ldg(CloverIO<PREC_HALF>::norms(clov, Vh_pad) + (size_t)parity * Vh_pad + s) * kInvFix;
+  auto w = [&](int k) { return CloverIO<PREC_HALF>::word(c, k); };
+  float2 ore[6], oim[6];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {  // diagonal words: (d_2q, d_2q+1) of each block
+    const float2 d0 = dec_lo2(w(q), w(18 + q)), d1 = dec_hi2(w(q), w(18 + q));
+    ore[2 * q] = fmul2(d0, v.re[2 * q]);
+    oim[2 * q] = fmul2(d0, v.im[2 * q]);
+    ore[2 * q + 1] = fmul2(d1, v.re[2 * q + 1]);
+    oim[2 * q + 1] = fmul2(d1, v.im[2 * q + 1]);
+  }
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      const int k = 3 + tri_index(i, j);
+      const float2 mre = dec_lo2(w(k), w(18 + k)), mim = dec_hi2(w(k), w(18 + k));
+      ore[i] = ffma2(mre, v.re[j], ore[i]);
+      ore[i] = ffma2(fneg2(mim), v.im[j], ore[i]);
+      oim[i] = ffma2(mre, v.im[j], oim[i]);
+      oim[i] = ffma2(mim, v.re[j], oim[i]);
+      ore[j] = ffma2(mre, v.re[i], ore[j]);
+      ore[j] = ffma2(mim, v.im[i], ore[j]);
+      oim[j] = ffma2(mre, v.im[i], oim[j]);
+      oim[j] = ffma2(fneg2(mim), v.re[i], oim[j]);
+    }
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    v.re[j] = fmul2(ore[j], splat2(nm));
+    v.im[j] = fmul2(oim[j], splat2(nm));
   }
 }
 

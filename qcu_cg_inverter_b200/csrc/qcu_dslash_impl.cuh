@@ -68,7 +68,8 @@ constexpr int dslash_minb(int op, int epi) {
   return op == OP_DOUBLE ? QCU_DSLASH_MINB64
          : op == OP_DOUBLE_BATCH ? QCU_DSLASH_MINB64_BATCH
          : op == OP_HALF_FAST_2 ? ((epi & EPI_OUT2) ? QCU_DSLASH_MINB_PAIR_OUT2 : QCU_DSLASH_MINB_PAIR)
-         : (op_spinor_prec(op) != PREC_HALF || (op == OP_HALF_FAST_1 && !QCU_DSLASH_CAP_1RHS)) ? QCU_DSLASH_MINB
+         : (op_spinor_prec(op) != PREC_HALF || ((op == OP_HALF_FAST_1 || op == OP_HALF_1) && !QCU_DSLASH_CAP_1RHS))
+             ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
          : (epi & EPI_CGXR)              ? QCU_DSLASH_MINB16_CGXR
          : (epi == EPI_CPRE)             ? QCU_DSLASH_MINB16_CPRE
@@ -101,30 +102,42 @@ QCU_D const void* clover_of(const DslashArgs& a, int r) {
 #include "qcu_dslash_pair.cuh"
 namespace qcu {
 
-// One output site and RHS of the fast 16-bit operator (16-bit spinors, FP32
-// 18-real links, FP32 block-interleaved clover): the hop and every epilogue in
-// block-paired FP32 instructions. Same arithmetic per component as the
-// generic body below; the norms are summed in FP32 before the FP64 block sums.
-template <bool DAG, int EPI>
+// v <- C v, block-paired, for the clover storage of link format PL's operator
+// (FP32 block-interleaved with the 18-real links, 16-bit with the 16-bit links)
+template <int PL>
+QCU_D void clover_block(SpinBlock& v, const void* clov, int Vh_pad, int parity, int s) {
+  if constexpr (PL == LINK_HALF_RAW)
+    clover_apply_block16(v, clov, Vh_pad, parity, s);
+  else
+    clover_apply_block(v, clov, Vh_pad, parity, s);
+}
+
+// One output site and RHS of a single-RHS 16-bit operator: the hop and every
+// epilogue in block-paired FP32 instructions. PL = LINK_SINGLE18: the fast
+// storage (FP32 18-real links, FP32 block-interleaved clover); PL =
+// LINK_HALF_RAW: the compact one (16-bit 12-real links, 16-bit clover). Same
+// arithmetic per component as the generic body below; the norms are summed in
+// FP32 before the FP64 block sums.
+template <int PL, bool DAG, int EPI>
 QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
   SpinBlock o;
-  hop_half_block<LINK_SINGLE18, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (float)a.bc_t);
+  hop_half_block<PL, DAG>(o, a.g, a.parity, s, r, a.in, a.gauge, (float)a.bc_t);
   const void* clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) ? clover_of(a, r) : nullptr;
   if (EPI & EPI_CPRE)
-    if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+    if (clov) clover_block<PL>(o, clov, a.g.Vh_pad, a.parity, s);
   if (EPI & EPI_XPAY) {
     const float2 c = splat2(a.coef ? (float)a.coef[r] : (float)a.coef0);
     SpinBlock xv;
     load16_block(xv, a.x, s, r);
     if (EPI & EPI_CX)
-      if (clov) clover_apply_block(xv, clov, a.g.Vh_pad, a.parity, s);
+      if (clov) clover_block<PL>(xv, clov, a.g.Vh_pad, a.parity, s);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
       o.re[j] = ffma2(c, o.re[j], xv.re[j]);
       o.im[j] = ffma2(c, o.im[j], xv.im[j]);
     }
     if (EPI & EPI_CPOST)
-      if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+      if (clov) clover_block<PL>(o, clov, a.g.Vh_pad, a.parity, s);
   }
   if constexpr ((EPI & EPI_CGXR) != 0) {
     // x += alpha p, r -= alpha out (the out of this kernel is the CG's z)
@@ -152,7 +165,7 @@ QCU_D void site_half_fast(const DslashArgs& a, int s, int r, double& nrm) {
     if (EPI & EPI_NORM) nrm = norm2_block(o);
   }
   if (EPI & EPI_OUT2) {
-    if (clov) clover_apply_block(o, clov, a.g.Vh_pad, a.parity, s);
+    if (clov) clover_block<PL>(o, clov, a.g.Vh_pad, a.parity, s);
     store16_block(a.out2, s, r, o);
   }
 }
@@ -170,7 +183,9 @@ QCU_D void dslash_site_body(const DslashArgs& a) {
   // (measured: 16^3x32 solve 3.70 vs 3.88 ms); with many RHS per launch the
   // generic body at the 85-register cap is faster (48-RHS batch 0.592 vs 0.606 s)
   if (OP == OP_HALF_FAST_1 && valid) {
-    site_half_fast<DAG, EPI>(a, s, r, nrm);
+    site_half_fast<LINK_SINGLE18, DAG, EPI>(a, s, r, nrm);
+  } else if (OP == OP_HALF_1 && valid) {
+    site_half_fast<LINK_HALF_RAW, DAG, EPI>(a, s, r, nrm);
   } else if (valid) {
     Spinor<R> o;
     hop<PS, PL, DAG, OP == OP_DOUBLE_BATCH>(o, a.g, a.parity, s, r, a.in, a.gauge, (R)a.bc_t);

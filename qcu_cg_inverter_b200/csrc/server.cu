@@ -155,7 +155,7 @@ int make_resident(qcu_server_s* s, int id) {
   int st = ctx_set_stream_priority(ctx, priority_for(s, R));
   if (st == QCU_SUCCESS) st = qcuGenerateGauge(ctx, R.seed, R.eps);
   if (st == QCU_SUCCESS) st = ctx_clover_reserve(ctx, s->P.clover_slots);
-  if (st == QCU_SUCCESS && s->P.autotune && !ctx_is_tuned(ctx, ctx_op(ctx, s->P.precision), s->P.columns))
+  if (st == QCU_SUCCESS && s->P.autotune && !ctx_is_tuned(ctx, ctx_op(ctx, s->P.precision, s->P.columns), s->P.columns))
     st = ctx_autotune(ctx, s->P.precision, s->P.columns, nullptr);
   std::unique_ptr<Engine> eng(new Engine());
   if (st == QCU_SUCCESS) {

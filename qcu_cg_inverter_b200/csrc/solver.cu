@@ -95,10 +95,10 @@ int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clove
   cudaStream_t st = ctx->stream;
   const int pa = acc_prec(ps);
   const int vp = ctx->g.Vh_pad;
-  if (w.nrhs != nrhs || w.ps != ps || w.op != ctx_op(ctx, ps) || w.vh_pad != vp || w.graph_gen != ctx->clover_gen) w.drop_graphs();
+  if (w.nrhs != nrhs || w.ps != ps || w.op != ctx_op(ctx, ps, nrhs) || w.vh_pad != vp || w.graph_gen != ctx->clover_gen) w.drop_graphs();
   w.graph_gen = ctx->clover_gen;
   w.clover = clover;
-  LaunchShape sh = ctx_shape(ctx, ctx_op(ctx, ps), nrhs);
+  LaunchShape sh = ctx_shape(ctx, ctx_op(ctx, ps, nrhs), nrhs);
   if (sh.Rb != w.shape.Rb || sh.Sb != w.shape.Sb) w.drop_graphs();
   w.shape = sh;
   QCU_CHECK(w.b2.alloc(PREC_DOUBLE, vp, nrhs, 2, st));
@@ -115,7 +115,7 @@ int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clove
   }
   w.nrhs = nrhs;
   w.ps = ps;
-  w.op = ctx_op(ctx, ps);
+  w.op = ctx_op(ctx, ps, nrhs);
   w.pa = pa;
   w.vh_pad = vp;
   w.st.rr = w.dd(D_RR);

@@ -55,7 +55,7 @@ bool ctx_is_tuned(qcu_context ctx, int prec, int nrhs) {
 int ctx_autotune(qcu_context ctx, int spinor_prec, int nrhs, double* best_ms) {
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
-  const int op = ctx_op(ctx, spinor_prec);
+  const int op = ctx_op(ctx, spinor_prec, nrhs);
   const int prec = op_spinor_prec(op);
   if (!ctx->gauge_loaded) {
     set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
@@ -148,7 +148,7 @@ extern "C" int qcuAutotune(qcu_context ctx, int precision, int nrhs, int* rhs_la
     return QCU_ERR_INVALID_ARG;
   }
   QCU_CHECK(ctx_autotune(ctx, precision, nrhs, ms));
-  LaunchShape sh = ctx_shape(ctx, ctx_op(ctx, precision), nrhs);
+  LaunchShape sh = ctx_shape(ctx, ctx_op(ctx, precision, nrhs), nrhs);
   if (rhs_lanes) *rhs_lanes = sh.Rb;
   if (site_lanes) *site_lanes = sh.Sb;
   return QCU_SUCCESS;
