@@ -57,8 +57,8 @@ ROOF_LATTICE = (32, 32, 32, 64)
 # DRAM bytes (read + write) per output site of the fused 16-bit stencil, per
 # storage of links and clover, from ncu captures of one launch (the traffic
 # grows with the number of sites): FP32 links and clover at 32^4 (592.9 MB for
-# 524288 sites)
-ROOF_TRAFFIC_BYTES_PER_SITE = {"fast": 592.9e6 / 524288, "compact": None}
+# 524288 sites); 16-bit links and clover at 32^3x64 (561.1 MB for 1048576 sites)
+ROOF_TRAFFIC_BYTES_PER_SITE = {"fast": 592.9e6 / 524288, "compact": 561.1e6 / 1048576}
 # storage behind the 16-bit solves (qcuContextSetHalfOperator) and its description
 STORAGE = {"auto": None, "fast": True, "compact": False}
 DTYPE = {"fast": "f32 arithmetic; 16-bit spinors, FP32 links (18 reals) and FP32 clover; f64 reliable updates",

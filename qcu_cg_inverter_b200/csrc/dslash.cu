@@ -40,6 +40,16 @@ DslashKernelFn pick_f16c1(bool dag, int epi, int fin);
 #define QCU_COMPACT_1RHS 1
 #endif
 
+// Batched launches on a one-dimensional grid with the RHS tiles of each site
+// tile adjacent (1), or on the (site tile, RHS tile) grid (0). Measured on
+// B200, 24^3x48 with 48 RHS (6 RHS tiles of 8): the fused CG stencil K2 2167
+// -> 1967 us (DRAM reads 3.93 -> 3.22 GB: the links and clover of a site tile
+// come from DRAM once instead of once per RHS tile), the CG update stencil
+// 1844 -> 1757 us, the 48-RHS batch 0.477 -> 0.455 s.
+#ifndef QCU_SLAB_MINOR
+#define QCU_SLAB_MINOR 1
+#endif
+
 static int g_pairs_override = -1;
 void set_rhs_pairs_override(int v) { g_pairs_override = v; }
 
@@ -72,8 +82,18 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
   if (sh.Rb < 1 || sh.Rb > 32 || (32 % sh.Rb) != 0 || (tx * sh.Sb) % 32 != 0 || sh.Rb * sh.Sb > 256)
     return cudaErrorInvalidConfiguration;
   dim3 block(tx, sh.Sb);
-  dim3 grid(grid_x(a.g.Vh, sh.Sb), (a.nrhs + sh.Rb - 1) / sh.Rb);
-  fn<<<grid, block, 0, stream>>>(a);
+  const int nslab = (a.nrhs + sh.Rb - 1) / sh.Rb;
+  if (QCU_SLAB_MINOR && nslab > 1) {
+    // the RHS tiles of one site tile run back to back, so its links and
+    // clover are read from DRAM once and served from L2 to the others
+    DslashArgs b = a;
+    b.nslab = nslab;
+    fn<<<dim3(grid_x(a.g.Vh, sh.Sb) * nslab, 1), block, 0, stream>>>(b);
+  } else {
+    DslashArgs b = a;
+    b.nslab = 0;
+    fn<<<dim3(grid_x(a.g.Vh, sh.Sb), nslab), block, 0, stream>>>(b);
+  }
   return cudaGetLastError();
 }
 

@@ -175,8 +175,9 @@ template <int OP, bool DAG, int EPI, class Fin>
 QCU_D void dslash_site_body(const DslashArgs& a) {
   constexpr int PS = op_spinor_prec(OP), PL = op_link_format(OP), PC = op_clover_prec(OP);
   typedef typename CompReal<PS>::type R;
-  const int r = blockIdx.y * blockDim.x + threadIdx.x;
-  const int s = blockIdx.x * blockDim.y + threadIdx.y;
+  const TileCoord tc = stencil_tile(a);
+  const int r = tc.rhs * blockDim.x + threadIdx.x;
+  const int s = tc.site * blockDim.y + threadIdx.y;
   const bool valid = (s < a.g.Vh) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
   double nrm = 0.0;
   // single-RHS launches of the fast 16-bit operator: block-paired epilogues
@@ -234,7 +235,7 @@ QCU_D void dslash_site_body(const DslashArgs& a) {
   }
   if (EPI & (EPI_NORM | EPI_CGXR)) {
     double v[1] = {nrm};
-    block_reduce_finish<1, Fin>(v, a.nrhs, a.red);
+    block_reduce_finish<1, Fin>(v, a.nrhs, a.red, tc);
   }
 }
 

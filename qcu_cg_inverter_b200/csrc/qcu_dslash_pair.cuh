@@ -369,13 +369,14 @@ QCU_D void xpay16_rp(PairSpinor& o, const CSpinorView& f, int s, RhsPair rp, flo
   }
 }
 
-// The kernel body: thread (threadIdx.x, threadIdx.y) serves RHS pair
-// 2*(blockIdx.y*blockDim.x + threadIdx.x) + {0, 1} of site
-// blockIdx.x*blockDim.y + threadIdx.y.
+// The kernel body: thread (threadIdx.x, threadIdx.y) of the block at tile
+// (site tile, RHS tile) serves RHS pair 2*(RHS tile*blockDim.x + threadIdx.x)
+// + {0, 1} of site (site tile)*blockDim.y + threadIdx.y.
 template <bool DAG, int EPI, class Fin>
 QCU_D void dslash_pair_body(const DslashArgs& a) {
-  const int r0 = 2 * (blockIdx.y * blockDim.x + threadIdx.x);
-  const int s = blockIdx.x * blockDim.y + threadIdx.y;
+  const TileCoord tc = stencil_tile(a);
+  const int r0 = 2 * (tc.rhs * blockDim.x + threadIdx.x);
+  const int s = tc.site * blockDim.y + threadIdx.y;
   const bool site_ok = s < a.g.Vh;
   const bool has1 = r0 + 1 < a.nrhs;
   const bool v0 = site_ok && r0 < a.nrhs && (a.active == nullptr || a.active[r0]);
@@ -424,7 +425,7 @@ QCU_D void dslash_pair_body(const DslashArgs& a) {
   }
   if (EPI & (EPI_NORM | EPI_CGXR)) {
     double v[2] = {n0, n1};
-    block_reduce_finish<1, Fin, 2>(v, a.nrhs, a.red);
+    block_reduce_finish<1, Fin, 2>(v, a.nrhs, a.red, tc);
   }
 }
 

@@ -44,6 +44,10 @@ struct DslashArgs {
   double coef0;
   double bc_t;
   const int* active;     // per-RHS mask, nullptr -> all active
+  // RHS tiles per site tile when the grid is one-dimensional with the RHS
+  // tiles of a site tile adjacent (blockIdx.x = site tile * nslab + RHS tile);
+  // 0: two-dimensional grid (blockIdx.x site tile, blockIdx.y RHS tile)
+  int nslab;
   ReduceArgs red;
   // EPI_CGXR: solution and residual in the accumulator precision (double for
   // FP64 spinors, else single), search direction in the spinor precision
@@ -70,5 +74,14 @@ void set_rhs_pairs_override(int v);
 
 // Number of blocks along x for a field of Vh sites.
 inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }
+
+// The (site tile, RHS tile) of this block of a stencil launch.
+QCU_D TileCoord stencil_tile(const DslashArgs& a) {
+  if (a.nslab > 0) {
+    const int st = blockIdx.x / a.nslab;
+    return TileCoord{st, (int)(gridDim.x / a.nslab), (int)(blockIdx.x - st * a.nslab)};
+  }
+  return TileCoord::from_grid();
+}
 
 }  // namespace qcu

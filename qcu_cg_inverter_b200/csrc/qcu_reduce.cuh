@@ -30,11 +30,19 @@ struct FinNone {
 // for that (smaller arrays leave more of the SM's memory to the L1 cache)
 constexpr int kMaxWarps = 8;
 
+// The block's place in a (site tile, RHS tile) launch grid: by default
+// blockIdx.x / gridDim.x over site tiles and blockIdx.y over RHS tiles.
+struct TileCoord {
+  int site, nsite, rhs;
+  static QCU_D TileCoord from_grid() { return TileCoord{(int)blockIdx.x, (int)gridDim.x, (int)blockIdx.y}; }
+};
+
 // vals: NR values for each of the RL right-hand sides of this thread (RHS
-// (blockIdx.y*Rb + threadIdx.x)*RL + j holds vals[j*NR .. j*NR+NR-1]; zero for
-// idle threads). Every thread of the block must call this.
+// (t.rhs*Rb + threadIdx.x)*RL + j holds vals[j*NR .. j*NR+NR-1]; zero for idle
+// threads). Every thread of the block must call this.
 template <int NR, class Fin, int RL = 1>
-QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs& red) {
+QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs& red,
+                               const TileCoord t = TileCoord::from_grid()) {
   __shared__ double sm[kMaxWarps][NR * RL * 32];
   __shared__ bool am_last;
   const int Rb = blockDim.x;
@@ -51,12 +59,12 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   __syncthreads();
   if (threadIdx.y == 0) {
     for (int j = 0; j < RL; j++) {
-      const int r = (blockIdx.y * Rb + threadIdx.x) * RL + j;
+      const int r = (t.rhs * Rb + threadIdx.x) * RL + j;
       if (r < nrhs) {
         for (int k = 0; k < NR; k++) {
           double acc = 0.0;
           for (int w = 0; w < nwarps; w++) acc += sm[w][(j * NR + k) * 32 + threadIdx.x];
-          red.partial[(size_t)(r * NR + k) * gridDim.x + blockIdx.x] = acc;
+          red.partial[(size_t)(r * NR + k) * t.nsite + t.site] = acc;
         }
       }
     }
@@ -75,8 +83,8 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   const int nq = nrhs * NR;
   for (int q = warp; q < nq; q += nwarps) {
     double acc = 0.0;
-    const volatile double* p = red.partial + (size_t)q * gridDim.x;
-    for (int b = lane; b < (int)gridDim.x; b += 32) acc += p[b];
+    const volatile double* p = red.partial + (size_t)q * t.nsite;
+    for (int b = lane; b < t.nsite; b += 32) acc += p[b];
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (lane == 0) red.result[q] = acc;
   }
