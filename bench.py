@@ -772,9 +772,10 @@ def run_stencil(args):
         elif not args.no_autotune:  # else: the shape from QCU_TUNE_CACHE or the default
             c.autotune(args.precision, args.nrhs)
         ms, nbytes = c.bench_stencil(args.precision, args.variant, args.nrhs, args.iters)
+        storage = c.half_storage(args.nrhs)
     gbs = nbytes / (ms / 1e3) / 1e9
     print(json.dumps({"stencil": args.stencil, "precision": args.precision, "variant": args.variant,
-                      "storage": c.half_storage(args.nrhs),
+                      "storage": storage,
                       "nrhs": args.nrhs, "ms_per_launch": ms, "bytes_per_launch": nbytes, "GBps": gbs,
                       "frac": gbs / hbm, "peak_source": src}), flush=True)
 

@@ -92,6 +92,13 @@ typedef struct {
   int status;            /* QCU_SUCCESS, QCU_ERR_NOT_CONVERGED or QCU_ERR_BREAKDOWN */
   double true_residual;  /* |b - M x|/|b| of the returned x, evaluated in FP64 */
   double kappa;
+  double gbytes;         /* algorithmic bytes (1e9) the solve of this RHS moved: every stencil,
+                            clover and BLAS pass of its iterations, reliable updates, admission
+                            and retirement, each neighbour load counted, link and clover bytes
+                            divided by the RHS that share one load */
+  double seconds;        /* qcuInvert: device time of the whole call (shared by its RHS);
+                            0 in request-server reports (see qcuServerQuery's latency) */
+  double gbytes_per_s;   /* qcuInvert: the call's gbytes summed over its RHS / seconds; 0 otherwise */
 } qcu_solve_report;
 
 /* Fills params with the defaults: kappa 0.12, csw 0, bc_t -1, tol 1e-10,
@@ -259,6 +266,55 @@ qcu_context qcuLegacyContext(void);
  * pointers, lattice extents with Lx even; synchronous. */
 int qcuShiftVectorStorage(void* dst, const void* src, int direction, int Lx, int Ly, int Lz, int Lt);
 int qcuShiftGaugeStorage(void* dst, const void* src, int direction, int Lx, int Ly, int Lz, int Lt);
+
+/* ---- domain decomposition along t (several GPUs, one lattice) ----
+ * Replaces the reference's MPI communicator (src/qcu_communicator.cu:
+ * 1033-1268 halo exchange, 1603-1623 global sums), which splits the lattice
+ * over a process grid; here the split is along t only, one slab per rank
+ * (one process per GPU), the local time extent Lt / nranks even and the time
+ * slice (Lx/2 * Ly * Lz sites) a multiple of 32. Each parity block of every
+ * field of a slab context carries two ghost slices behind its sites; before a
+ * hop the slab's first and last slices are sent to the neighbouring ranks'
+ * ghost slices (into the receiver's own memory), and the solver's dot
+ * products are summed over the ranks. Fields given to a slab context are the
+ * rank's part of the global field: the slices t0 .. t0 + Lt/nranks - 1, t0 =
+ * rank * Lt/nranks, in the reference AoS layouts of that local lattice.
+ *
+ * Transports: NCCL (ncclSend/ncclRecv into the peers' ghost slices, and
+ * ncclAllReduce, all enqueued on the context's stream, so CUDA graphs capture
+ * them), or a host transport whose two callbacks move host buffers between
+ * ranks (for callers that bring their own messaging, as the reference's MPI
+ * host staging does; the library stages through pinned host memory and
+ * synchronises around each call, and solves on it run without CUDA graphs). */
+typedef struct qcu_comm_s* qcu_comm;
+/* Host transport: send send_lo (this rank's first slices) to rank - 1 and
+ * send_hi (its last slices) to rank + 1, receive rank + 1's send_lo into
+ * recv_hi and rank - 1's send_hi into recv_lo (ranks modulo nranks; all four
+ * buffers `bytes` long, host memory). Returns 0 on success. */
+typedef int (*qcu_exchange_fn)(void* user, const void* send_lo, const void* send_hi, void* recv_lo, void* recv_hi,
+                               size_t bytes);
+/* Host transport: values[0..n) <- their sum over all ranks. Returns 0 on success. */
+typedef int (*qcu_allreduce_fn)(void* user, double* values, int n);
+
+/* The NCCL unique id (bytes >= 128) rank 0 creates and every rank passes to
+ * qcuCommCreateNccl. */
+int qcuCommNcclUniqueId(void* id, int bytes);
+/* This process's rank of an NCCL communicator of nranks ranks on `device`. */
+int qcuCommCreateNccl(qcu_comm* comm, const void* id, int nranks, int rank, int device);
+int qcuCommCreateHost(qcu_comm* comm, int nranks, int rank, qcu_exchange_fn exchange, qcu_allreduce_fn allreduce,
+                      void* user);
+int qcuCommDestroy(qcu_comm comm);
+/* The slab of the comm's rank of the global lattice `lattice` on `device`.
+ * qcuLoadGauge / qcuGenerateGauge, qcuDslash, qcuApplyOperator and qcuInvert
+ * work on it with local fields; every rank makes the same calls in the same
+ * order. The context keeps an extended copy of its slab (two more slices on
+ * each side) for the clover term. Not for the request server or the
+ * reference-interface entry points. */
+int qcuContextCreateSlab(qcu_context* ctx, const int lattice[4], qcu_comm comm, int device);
+/* The slab geometry (host arithmetic only, no GPU): out = {t0, local Lt,
+ * slice sites, local half volume, first forward-ghost site, first
+ * backward-ghost site}; QCU_ERR_INVALID_ARG when the lattice does not split. */
+int qcuSlabGeometry(const int lattice[4], int nranks, int rank, int out[6]);
 
 /* Test hook for host-side fault injection: after n more successful device
  * allocations the next one fails as out-of-memory (n < 0 disables). */

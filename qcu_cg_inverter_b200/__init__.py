@@ -67,11 +67,17 @@ class ServerParams(ctypes.Structure):
 
 class SolveReport(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("converged", ctypes.c_int),
-                ("status", ctypes.c_int), ("true_residual", ctypes.c_double), ("kappa", ctypes.c_double)]
+                ("status", ctypes.c_int), ("true_residual", ctypes.c_double), ("kappa", ctypes.c_double),
+                ("gbytes", ctypes.c_double), ("seconds", ctypes.c_double), ("gbytes_per_s", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
+
+# host transport callbacks (include/qcu_b200.h qcu_exchange_fn, qcu_allreduce_fn)
+_EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_size_t)
+_ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int)
 
 _lib = None
 
@@ -149,6 +155,12 @@ def lib():
             "qcuServerPending": (i, [P]),
             "qcuServerDeviceBytes": (ll, [P]),
             "qcuHostAlloc": (P, [ll]),
+            "qcuSlabGeometry": (i, [ctypes.POINTER(i), i, i, ctypes.POINTER(i)]),
+            "qcuCommNcclUniqueId": (i, [P, i]),
+            "qcuCommCreateNccl": (i, [ctypes.POINTER(P), P, i, i, i]),
+            "qcuCommCreateHost": (i, [ctypes.POINTER(P), i, i, _EXCHANGE_FN, _ALLREDUCE_FN, P]),
+            "qcuCommDestroy": (i, [P]),
+            "qcuContextCreateSlab": (i, [ctypes.POINTER(P), ctypes.POINTER(i), P, i]),
             "qcuHostFree": (None, [P]),
         }
         for name, (res, args) in sig.items():
@@ -603,3 +615,149 @@ class Server:
     @property
     def device_bytes(self) -> int:
         return int(lib().qcuServerDeviceBytes(self._h))
+
+
+# ---------------------------------------------------------------------------
+# domain decomposition along t (include/qcu_b200.h, "domain decomposition")
+# ---------------------------------------------------------------------------
+def slab_geometry(lattice, nranks: int, rank: int) -> dict:
+    """The t-slab of `rank` of a lattice split over nranks ranks (host
+    arithmetic, no GPU): first global slice, local time extent, sites per
+    slice, local half volume and the first sites of the two ghost slices."""
+    L4 = (ctypes.c_int * 4)(*[int(v) for v in lattice])
+    out = (ctypes.c_int * 6)()
+    _check(lib().qcuSlabGeometry(L4, int(nranks), int(rank), out))
+    return dict(zip(("t0", "lt", "face", "vh", "ghost_fwd", "ghost_bwd"), list(out)))
+
+
+def _host_view(addr: int, nbytes: int):
+    import numpy as np
+    return np.ctypeslib.as_array((ctypes.c_ubyte * nbytes).from_address(addr))
+
+
+def dist_transport():
+    """The host transport's two callables over the default torch.distributed
+    process group (CPU tensors, e.g. gloo): each rank sends its first slices
+    to rank - 1 and its last ones to rank + 1 (tags tell the two streams
+    apart when both neighbours are the same rank), and sums in place."""
+    import torch
+    import torch.distributed as dist
+    rank, n = dist.get_rank(), dist.get_world_size()
+    lo, hi = (rank - 1) % n, (rank + 1) % n
+
+    def exchange(send_lo, send_hi, recv_lo, recv_hi):
+        if n == 1:
+            recv_hi[:] = send_lo
+            recv_lo[:] = send_hi
+            return
+        t = [torch.from_numpy(a) for a in (send_lo, send_hi, recv_lo, recv_hi)]
+        reqs = [dist.isend(t[0], lo, tag=1), dist.irecv(t[3], hi, tag=1),
+                dist.isend(t[1], hi, tag=2), dist.irecv(t[2], lo, tag=2)]
+        for r in reqs:
+            r.wait()
+
+    def allreduce(values):
+        dist.all_reduce(torch.from_numpy(values))
+
+    return exchange, allreduce
+
+
+class Comm:
+    """A communicator of the t-slab decomposition: NCCL (device buffers, the
+    context's stream, capturable by CUDA graphs) or a host transport driven by
+    two Python callables (the reference's host-staged exchange):
+
+        exchange(send_lo, send_hi, recv_lo, recv_hi)  # numpy uint8 views
+        allreduce(values)                             # numpy float64 view, summed in place
+
+    send_lo goes to rank - 1 (its recv_hi), send_hi to rank + 1 (its recv_lo)."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        self._keep = ()
+        self.nranks = self.rank = 0
+
+    @staticmethod
+    def nccl_unique_id() -> bytes:
+        buf = (ctypes.c_ubyte * 128)()
+        _check(lib().qcuCommNcclUniqueId(ctypes.cast(buf, ctypes.c_void_p), 128))
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, uid: bytes, nranks: int, rank: int, device: int = 0) -> "Comm":
+        c = cls()
+        buf = (ctypes.c_ubyte * 128).from_buffer_copy(uid)
+        _check(lib().qcuCommCreateNccl(ctypes.byref(c._h), ctypes.cast(buf, ctypes.c_void_p), int(nranks), int(rank),
+                                       int(device)))
+        c.nranks, c.rank = int(nranks), int(rank)
+        return c
+
+    @classmethod
+    def host(cls, nranks: int, rank: int, exchange=None, allreduce=None) -> "Comm":
+        c = cls()
+
+        def xfn(user, slo, shi, rlo, rhi, nbytes):
+            try:
+                exchange(_host_view(slo, nbytes), _host_view(shi, nbytes), _host_view(rlo, nbytes),
+                         _host_view(rhi, nbytes))
+                return 0
+            except Exception:  # reported to the library as a failed exchange
+                return 1
+
+        def rfn(user, values, n):
+            try:
+                import numpy as np
+                allreduce(np.ctypeslib.as_array(values, shape=(n,)))
+                return 0
+            except Exception:
+                return 1
+
+        cx = _EXCHANGE_FN(xfn) if exchange else _EXCHANGE_FN()
+        cr = _ALLREDUCE_FN(rfn) if allreduce else _ALLREDUCE_FN()
+        _check(lib().qcuCommCreateHost(ctypes.byref(c._h), int(nranks), int(rank), cx, cr, None))
+        c._keep = (cx, cr)  # the callbacks must outlive the communicator
+        c.nranks, c.rank = int(nranks), int(rank)
+        return c
+
+    @classmethod
+    def torch_distributed(cls, device: int = 0) -> "Comm":
+        """From the default torch.distributed process group: NCCL between the
+        GPUs when the group's backend is nccl (the unique id travels through
+        a broadcast), else the host transport over the group (gloo)."""
+        import torch
+        import torch.distributed as dist
+        rank, n = dist.get_rank(), dist.get_world_size()
+        if dist.get_backend() == "nccl":
+            obj = [cls.nccl_unique_id() if rank == 0 else None]
+            dist.broadcast_object_list(obj, src=0)
+            return cls.nccl(obj[0], n, rank, device)
+        exchange, allreduce = dist_transport()
+        return cls.host(n, rank, exchange, allreduce)
+
+    def close(self):
+        if self._h:
+            lib().qcuCommDestroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SlabContext(Context):
+    """The slab of this rank of a lattice decomposed along t. Same methods as
+    Context, on the rank's local fields (slices t0 .. t0 + lt - 1 of every
+    global field, reference AoS layouts of the local lattice); every rank
+    makes the same calls in the same order."""
+
+    def __init__(self, lattice, comm: Comm, device: int = 0):
+        geo = slab_geometry(lattice, comm.nranks, comm.rank)
+        self.global_lattice = tuple(int(v) for v in lattice)
+        self.lattice = self.global_lattice[:3] + (geo["lt"],)
+        self.t0 = geo["t0"]
+        self.comm = comm  # kept alive with the context
+        self._h = ctypes.c_void_p()
+        L4 = (ctypes.c_int * 4)(*self.global_lattice)
+        _check(lib().qcuContextCreateSlab(ctypes.byref(self._h), L4, comm._h, int(device)))

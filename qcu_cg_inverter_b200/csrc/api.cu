@@ -171,7 +171,8 @@ const void* ctx_gauge(qcu_context ctx, int op) {
   }
 }
 
-static int ingest_gauge(qcu_context ctx, const void* gauge) {
+int ingest_gauge(qcu_context ctx, const void* gauge) {
+  if (ctx->g.tdd) return dd_ingest_gauge(ctx, gauge);
   const Geom& g = ctx->g;
   QCU_CHECK(ctx->gauge64.ensure(gauge_field_bytes(PREC_DOUBLE, g.Vh_pad), ctx->stream));
   QCU_CHECK(ctx->gauge32.ensure(gauge_field_bytes(PREC_SINGLE, g.Vh_pad), ctx->stream));
@@ -252,6 +253,16 @@ int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot, bool wait) {
     QCU_CHECK(ctx_clover_reserve(ctx, B.capacity + 1));
     k = B.capacity - 1;
   }
+  if (ctx->ext) {  // a t-slab: built on the extended slab, its slices copied over
+    int es = -1;
+    QCU_CHECK(ctx_clover_slot(ctx->ext, csw_eff, &es, true));
+    QCU_CHECK(dd_clover_from_ext(ctx, es, k));
+    QCU_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    B.csw[k] = csw_eff;
+    B.stamp[k] = ++ctx->clock;
+    *slot = k;
+    return QCU_SUCCESS;
+  }
   QCU_CHECK(ctx->status.ensure(64, ctx->stream));
   QCU_CHECK_CUDA(cudaMemsetAsync(ctx->status.p, 0, 64, ctx->stream));
   QCU_CHECK_CUDA(launch_clover_build(ctx->g, ctx->gauge64.p, csw_eff, static_cast<char*>(B.A64.p) + B.b64 * k,
@@ -319,6 +330,7 @@ static DslashArgs base_args(qcu_context ctx, int prec) {
 }
 
 static int run_dslash(qcu_context ctx, int prec, bool dag, int epi, const DslashArgs& a) {
+  QCU_CHECK(dd_exchange(ctx, a.in, op_spinor_prec(prec), ctx->stream));  // t-slab: the neighbours' faces
   QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, FIN_NONE, a, ctx->shape1, ctx->stream));
   ctx->launches++;
   return QCU_SUCCESS;
@@ -511,6 +523,7 @@ int qcuContextDestroy(qcu_context ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   qcu_solver_workspace_free(ctx);
+  if (ctx->ext) qcuContextDestroy(ctx->ext);
   delete ctx;
   return QCU_SUCCESS;
 }
@@ -552,10 +565,11 @@ int qcuContextSetHalfOperator(qcu_context ctx, int fast_links) {
 
 int qcuContextHalfOperator(qcu_context ctx, int nrhs) {
   clear_error();
-  QCU_CHECK(ctx_check(ctx));
+  const int st = ctx_check(ctx);
+  if (st != QCU_SUCCESS) return -st;
   if (nrhs < 1) {
     set_error(QCU_ERR_INVALID_ARG, "nrhs must be positive");
-    return QCU_ERR_INVALID_ARG;
+    return -QCU_ERR_INVALID_ARG;
   }
   return ctx_op(ctx, PREC_HALF, nrhs) == OP_HALF ? 0 : 1;
 }
@@ -590,6 +604,7 @@ int qcuLoadGauge(qcu_context ctx, const void* gauge) {
 int qcuGenerateGauge(qcu_context ctx, unsigned long long seed, double eps) {
   clear_error();
   QCU_CHECK(ctx_check(ctx));
+  if (ctx->g.tdd) return dd_generate_gauge(ctx, seed, eps);
   size_t aos_bytes = (size_t)8 * ctx->g.Vh * 9 * 16;
   DevBuf tmp;
   QCU_CHECK(tmp.ensure(aos_bytes, ctx->stream));
@@ -618,7 +633,11 @@ int qcuGenerateSpinor(qcu_context ctx, void* out, int nrhs, unsigned long long s
     dst = ctx->stage_out.p;
   }
   for (int r = 0; r < nrhs; r++) {
-    QCU_CHECK_CUDA(launch_spinor_random(per, seed + r, static_cast<char*>(dst) + per * 192 * r, ctx->stream));
+    char* d = static_cast<char*>(dst) + per * 192 * r;
+    if (ctx->g.tdd)  // the slab's part of the global field's spinor
+      QCU_CHECK_CUDA(launch_spinor_random_slab(ctx->g, ctx->Lt_global, ctx->t0, seed + r, d, ctx->stream));
+    else
+      QCU_CHECK_CUDA(launch_spinor_random(per, seed + r, d, ctx->stream));
     ctx->launches++;
   }
   if (!dev) QCU_CHECK_CUDA(cudaMemcpyAsync(out, dst, per * 192 * nrhs, cudaMemcpyDeviceToHost, ctx->stream));
@@ -748,6 +767,7 @@ void loadQcuGauge(void* gauge, QcuParam* param) {
 }
 
 void dslashQcu(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int parity) {
+  NvtxRange nv("dslashQcu");
   std::lock_guard<std::mutex> lk(g_legacy_mu);
   qcu_context ctx;
   if (legacy_begin(param, gauge, &ctx) != QCU_SUCCESS) return;
@@ -766,6 +786,7 @@ static int legacy_full(qcu_context ctx, void* out, void* in, int kind, int dag) 
 }
 
 void fullDslashQcu(void* fermion_out, void* fermion_in, void* gauge, QcuParam* param, int dagger_flag) {
+  NvtxRange nv("fullDslashQcu");
   std::lock_guard<std::mutex> lk(g_legacy_mu);
   qcu_context ctx;
   if (legacy_begin(param, gauge, &ctx) != QCU_SUCCESS) return;
@@ -937,6 +958,7 @@ static int ref_cg(qcu_context ctx, void* b_vec, void* x_vec, int* iters_out, boo
 extern "C" {
 
 void cg_inverter(void* b_vector, void* x_vector, void* gauge, QcuParam* param) {
+  NvtxRange nv("cg_inverter");
   std::lock_guard<std::mutex> lk(g_legacy_mu);
   qcu_context ctx;
   if (legacy_begin(param, gauge, &ctx) != QCU_SUCCESS) return;

@@ -175,6 +175,10 @@ extern "C" int qcuDebugStencil(qcu_context ctx, int prec, int dagger, int epi, i
     set_error(QCU_ERR_NOT_INITIALIZED, "no gauge field loaded");
     return QCU_ERR_NOT_INITIALIZED;
   }
+  if (ctx->g.tdd) {
+    set_error(QCU_ERR_UNSUPPORTED, "qcuDebugStencil runs on whole-lattice contexts only");
+    return QCU_ERR_UNSUPPORTED;
+  }
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   const int op = ctx_op(ctx, prec, nrhs);

@@ -8,6 +8,8 @@
 #include <memory>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "qcu_engine.h"
 
 // Chunk sizing knobs, measured on B200 (16^3x32 solves, kernels per solve):
@@ -177,6 +179,7 @@ long long Engine::device_bytes() const {
 // Source in, |b|, bhat = A_ee^-1 (b_e + kappa D_eo A_oo^-1 b_o), x = 0 and
 // p = 0, for every column admitted since the last step.
 int Engine::enqueue_admissions() {
+  NvtxRange nv("qcu admissions");
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   const OpCtx o = op();
@@ -198,7 +201,14 @@ int Engine::enqueue_admissions() {
   const int* adm = w.di(I_ADM);
   {
     ReduceArgs ra = red_into(o, ctx->red.result.as<double>(), false);
+    if (g.tdd) {  // the sum runs over both parity blocks whole: their ghost slices must hold zeros
+      const size_t per = (size_t)12 * 16 * cap;
+      for (int p = 0; p < 2; p++)
+        QCU_CHECK_CUDA(cudaMemsetAsync(w.b2.data.as<char>() + p * w.b2.parity_bytes() + g.gfwd * per, 0,
+                                       (size_t)2 * g.st * per, st));
+    }
     QCU_CHECK_CUDA(launch_cdot(PREC_DOUBLE, 2 * g.Vh_pad, cap, w.b2.cview(0), w.b2.cview(0), adm, ra, w.shape, st));
+    QCU_CHECK(dd_sum(ctx, ctx->red.result.as<double>(), 2 * cap, st));
     slot_bnorm_kernel<<<nb32(cap), 32, 0, st>>>(cap, w.mem.as<double>(), w.di(0), ctx->red.result.as<double>());
     QCU_CHECK_CUDA(cudaGetLastError());
     ctx->launches += 2;
@@ -264,7 +274,11 @@ int Engine::chunk_length() const {
   return (int)std::max(1.0, std::min(ceil(need), (double)std::max(1, P.max_chunk)));
 }
 
+NvtxRange::NvtxRange(const char* name) { nvtxRangePushA(name); }
+NvtxRange::~NvtxRange() { nvtxRangePop(); }
+
 int Engine::step(bool* launched) {
+  NvtxRange nv("qcu engine step");
   *launched = false;
   if (pending.empty() && live.empty()) return QCU_SUCCESS;
   if (w.graph_gen != ctx->clover_gen) {  // the clover bank moved
@@ -384,6 +398,15 @@ int Engine::observe(std::vector<Group*>* retired) {
       rep.status = conv ? QCU_SUCCESS : (stat != QCU_SUCCESS ? stat : QCU_ERR_NOT_CONVERGED);
       rep.true_residual = w.hd(D_TRUE)[r];
       rep.kappa = q->kappa;
+      {
+        const int share = cap > 1 ? w.shape.Rb : 1;  // RHS served by one link / clover load
+        const double per_site = rep.iterations * iteration_bytes(w.op, P.clover, share) +
+                                rep.reliable_updates * reliable_update_bytes(w.op, P.clover, share) +
+                                admit_retire_bytes(P.clover, share);
+        rep.gbytes = per_site * ctx->g.Vh * 1e-9;
+        rep.seconds = 0.0;
+        rep.gbytes_per_s = 0.0;
+      }
       if (rep.status != QCU_SUCCESS && (worst == QCU_SUCCESS || rep.status == QCU_ERR_INVALID_ARG)) worst = rep.status;
     }
     q->status = worst;
@@ -403,6 +426,7 @@ int Engine::observe(std::vector<Group*>* retired) {
 // x_e += x_lo, x_o = A_oo^-1 (b_o + kappa D_oe x_e), both halves out in the
 // AoS layout, and the solution copied to the caller's buffer.
 int Engine::enqueue_retirement(const std::vector<Group*>& gs) {
+  NvtxRange nv("qcu retirement");
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   const OpCtx o = op();
@@ -454,6 +478,7 @@ extern "C" long long qcu_engine_device_bytes(qcu_context ctx) {
 
 extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, const double* kappas,
                          const qcu_solve_params* params, qcu_solve_report* reports) {
+  NvtxRange nv("qcuInvert");
   clear_error();
   QCU_CHECK(ctx_check(ctx));
   if (!x || !b || nrhs < 1 || !params) {
@@ -488,6 +513,17 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
     QCU_CHECK(ctx_autotune(ctx, P.precision, nrhs, nullptr));
   if (!ctx->engine) ctx->engine = new Engine();
   Engine& E = *ctx->engine;
+  // device time of the call (every admission, step and retirement), for the reports
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess) {
+    if (t0) cudaEventDestroy(t0);
+    return cuda_status(cudaGetLastError(), "cudaEventCreate");
+  }
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } ev_guard{t0, t1};
+  QCU_CHECK_CUDA(cudaEventRecord(t0, ctx->stream));
   EngineParams ep;
   ep.precision = P.precision;
   ep.bc_t = P.bc_t;
@@ -495,7 +531,7 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
   ep.delta = P.delta;
   ep.maxiter = P.maxiter;
   ep.clover = clover;
-  ep.graphs = P.use_graphs != 0;
+  ep.graphs = P.use_graphs != 0 && dd_graphs_ok(ctx);
   QCU_CHECK(E.configure(ctx, nrhs, ep));
   // one group per run of equal kappa
   const bool bdev = is_device_ptr(b), xdev = is_device_ptr(x);
@@ -535,11 +571,21 @@ extern "C" int qcuInvert(qcu_context ctx, void* x, const void* b, int nrhs, cons
     E.abort();
     return st;
   }
+  QCU_CHECK_CUDA(cudaEventRecord(t1, ctx->stream));
   QCU_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  QCU_CHECK_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  double total_gb = 0.0;
+  for (auto& q : groups)
+    for (int i = 0; i < q->n; i++) total_gb += q->reports[i].gbytes;
+  const double secs = ms * 1e-3;
   int ret = QCU_SUCCESS;
   for (auto& q : groups) {
-    for (int i = 0; i < q->n; i++)
+    for (int i = 0; i < q->n; i++) {
+      q->reports[i].seconds = secs;
+      q->reports[i].gbytes_per_s = secs > 0 ? total_gb / secs : 0.0;
       if (reports) reports[q->tag + i] = q->reports[i];
+    }
     if (q->status == QCU_ERR_INVALID_ARG) ret = QCU_ERR_INVALID_ARG;
     else if (q->status != QCU_SUCCESS && ret == QCU_SUCCESS) ret = q->status;
   }

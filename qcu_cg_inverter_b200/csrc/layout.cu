@@ -232,6 +232,54 @@ __global__ void spinor_random_kernel(size_t nsites, uint64_t seed, double2* out)
   }
 }
 
+// The links of slices t_first .. t_first + nslices - 1 (modulo the global
+// time extent) of the global lattice's seeded field: link l of this slab has
+// the stream of the global link with the same direction, parity and spatial
+// site, so the union of the slabs is the field launch_gauge_random makes for
+// the whole lattice.
+__global__ void gauge_random_slab_kernel(size_t nlinks, size_t vh, size_t face, size_t vh_glob, int lt_glob,
+                                         int t_first, uint64_t seed, double eps, double2* out) {
+  size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nlinks) return;
+  const size_t mp = l / vh, s = l - mp * vh;
+  const size_t ts = s / face, rest = s - ts * face;
+  const int tg = (int)(((long long)t_first + (long long)ts) % lt_glob + lt_glob) % lt_glob;
+  uint64_t st = stream_init(seed, mp * vh_glob + (size_t)tg * face + rest);
+  C64 u[9];
+  su3_from_stream(u, st, eps);
+  for (int i = 0; i < 9; i++) out[l * 9 + i] = make_double2(u[i].re, u[i].im);
+}
+
+cudaError_t launch_gauge_random_slab(const Geom& g, int lt_glob, int t_first, uint64_t seed, double eps, void* aos,
+                                     cudaStream_t st) {
+  const size_t n = (size_t)8 * g.Vh, face = (size_t)g.st;
+  gauge_random_slab_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, g.Vh, face, face * lt_glob, lt_glob,
+                                                                          t_first, seed, eps, static_cast<double2*>(aos));
+  return cudaGetLastError();
+}
+
+// One full spinor of a slab (both parities, vh sites each) with the streams
+// of the global field's sites: site s of parity p is global site
+// p * vh_glob + offset + s.
+__global__ void spinor_random_slab_kernel(size_t vh, size_t vh_glob, size_t offset, uint64_t seed, double2* out) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * vh) return;
+  const size_t p = i / vh, s = i - p * vh;
+  uint64_t st = stream_init(seed ^ 0xA0761D6478BD642Full, p * vh_glob + offset + s);
+  for (int k = 0; k < 12; k++) {
+    double a, b;
+    gauss2(st, a, b);
+    out[i * 12 + k] = make_double2(a, b);
+  }
+}
+
+cudaError_t launch_spinor_random_slab(const Geom& g, int lt_glob, int t0, uint64_t seed, void* aos, cudaStream_t st) {
+  const size_t n = (size_t)2 * g.Vh, face = (size_t)g.st;
+  spinor_random_slab_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g.Vh, face * lt_glob, face * t0, seed,
+                                                                           static_cast<double2*>(aos));
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gauge_random(const Geom& g, uint64_t seed, double eps, void* aos, cudaStream_t st) {
   size_t n = (size_t)8 * g.Vh;
   gauge_random_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(n, seed, eps, static_cast<double2*>(aos));

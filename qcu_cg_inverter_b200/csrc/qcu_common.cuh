@@ -103,9 +103,17 @@ struct Geom {
   int Lx, Ly, Lz, Lt;
   int Lxh;      // Lx/2
   int Vh;       // sites per parity
-  int Vh_pad;   // Vh rounded up to the 32-site block
+  int Vh_pad;   // sites per parity block of every field: Vh rounded up to the 32-site block, plus the ghost slices
   int sy, sz, st;  // checkerboard strides of y, z, t: Lxh, Lxh*Ly, Lxh*Ly*Lz
   FastDiv dxh, dy, dz;  // division by Lxh, Ly, Lz
+  // t-slab of a lattice decomposed along t (tdd = 1): the hops across the
+  // slab's t faces read ghost slices appended to every parity block, the
+  // forward one at sites [gfwd, gfwd + st), the backward one at [gbwd, gbwd +
+  // st), filled by the halo exchange; tdd = 0: periodic wrap inside the lattice
+  int tdd, gfwd, gbwd;
+  // which t faces are the lattice's boundary, where hops take the factor bc_t:
+  // bit 0 the backward face (t = 0), bit 1 the forward one (t = Lt - 1)
+  int tbc;
 };
 
 inline Geom make_geom(const int L[4]) {
@@ -120,6 +128,30 @@ inline Geom make_geom(const int L[4]) {
   g.dxh = make_fastdiv(g.Lxh);
   g.dy = make_fastdiv(g.Ly);
   g.dz = make_fastdiv(g.Lz);
+  g.tdd = 0;
+  g.gfwd = g.gbwd = 0;
+  g.tbc = 3;
+  return g;
+}
+
+// The slab of rank `rank` of `nranks` of a lattice decomposed along t: local
+// time extent L[3] / nranks (even, so that local and global parity agree),
+// ghost slices after the slab's sites. Needs the slice (Lxh*Ly*Lz sites) to be
+// a whole number of 32-site blocks, so that a slice is a contiguous range of
+// every field; slab_ok() checks that.
+inline bool slab_ok(const int L[4], int nranks) {
+  if (nranks < 1 || L[3] % nranks) return false;
+  const int lt = L[3] / nranks;
+  return lt >= 2 && lt % 2 == 0 && ((L[0] / 2) * L[1] * L[2]) % 32 == 0;
+}
+inline Geom make_geom_slab(const int L[4], int nranks, int rank) {
+  const int Ll[4] = {L[0], L[1], L[2], L[3] / nranks};
+  Geom g = make_geom(Ll);
+  g.tdd = 1;
+  g.gfwd = g.Vh;  // a multiple of 32 (slab_ok)
+  g.gbwd = g.Vh + g.st;
+  g.Vh_pad = g.Vh + 2 * g.st;
+  g.tbc = (rank == 0 ? 1 : 0) | (rank == nranks - 1 ? 2 : 0);
   return g;
 }
 
@@ -129,7 +161,8 @@ inline Geom make_geom(const int L[4]) {
 // one x/2-1 when eo == parity; every direction wraps periodically.
 struct Nbrs {
   int fwd[4], bwd[4];
-  int t;   // time coordinate (for the t boundary phase)
+  int t;       // time coordinate
+  bool tf, tb;  // the forward / backward t hop crosses the lattice's boundary (takes bc_t)
 };
 
 QCU_HD Nbrs neighbours(const Geom& g, int s, int parity) {
@@ -150,8 +183,16 @@ QCU_HD Nbrs neighbours(const Geom& g, int s, int parity) {
   n.bwd[1] = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
   n.fwd[2] = (z + 1 == g.Lz) ? s - (g.Lz - 1) * g.sz : s + g.sz;
   n.bwd[2] = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
-  n.fwd[3] = (t + 1 == g.Lt) ? s - (g.Lt - 1) * g.st : s + g.st;
-  n.bwd[3] = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
+  const bool top = t + 1 == g.Lt, bot = t == 0;
+  n.tf = top && (g.tbc & 2);
+  n.tb = bot && (g.tbc & 1);
+  if (g.tdd) {  // across the slab's faces: the ghost slices
+    n.fwd[3] = top ? g.gfwd + (s - (g.Lt - 1) * g.st) : s + g.st;
+    n.bwd[3] = bot ? g.gbwd + s : s - g.st;
+  } else {
+    n.fwd[3] = top ? s - (g.Lt - 1) * g.st : s + g.st;
+    n.bwd[3] = bot ? s + (g.Lt - 1) * g.st : s - g.st;
+  }
   return n;
 }
 

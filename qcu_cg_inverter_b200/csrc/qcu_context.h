@@ -19,6 +19,15 @@
 
 namespace qcu {
 
+// NVTX range for the scope of a C entry point or a solver phase (visible in
+// nsys / ncu timelines; costs a few ns when no tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name);
+  ~NvtxRange();
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // ---------------- errors ----------------
 void set_error(int code, const std::string& msg);
 void clear_error();
@@ -140,6 +149,13 @@ struct qcu_context_s {
   bool tune_cache_loaded = false;
   long long clover_gen = 0;  // bumped whenever the clover bank moves
   long long launches = 0;
+  // t-slab of a decomposed lattice (comm.cu): the communicator, the global
+  // time extent and this slab's first global slice, and the extended slab
+  // (two more slices on each side, periodic) that ingests the gauge field and
+  // builds the clover term
+  qcu_comm comm = nullptr;
+  int Lt_global = 0, t0 = 0;
+  qcu_context ext = nullptr;
   ~qcu_context_s();
 };
 
@@ -187,6 +203,18 @@ bool is_device_ptr_on(const void* p, int device);
 int noalloc_prepare(int device);
 cudaError_t preload_spinor_io_f64();
 
+// t-slab decomposition (comm.cu): ghost slices of a spinor view of precision
+// `prec` from the neighbouring ranks, and global sums of n doubles in place
+// (both no-ops on a context that is not a slab)
+int dd_exchange(qcu_context ctx, const CSpinorView& v, int prec, cudaStream_t st);
+int dd_sum(qcu_context ctx, double* values, int n, cudaStream_t st);
+// copies the slab's part of the extended slab's clover slot into its own slot
+int dd_clover_from_ext(qcu_context ctx, int ext_slot, int slot);
+// the finishing functor `fin` (FinId) applied to reduced totals, as the
+// reduction's last block would have (solver.cu)
+cudaError_t launch_fin(int fin, const ReduceArgs& red, int nrhs, cudaStream_t st);
+bool dd_graphs_ok(qcu_context ctx);
+
 // kernel launchers (defined in the .cu files)
 cudaError_t launch_gauge_ingest(const Geom& g, const void* aos, void* d64, void* d32, void* d16, void* d18,
                                 cudaStream_t st);
@@ -198,6 +226,17 @@ cudaError_t launch_spinor_out(int prec, const Geom& g, int count, CSpinorView sr
                               cudaStream_t st, int r0 = 0);
 cudaError_t launch_gauge_random(const Geom& g, uint64_t seed, double eps, void* aos, cudaStream_t st);
 cudaError_t launch_spinor_random(size_t nsites, uint64_t seed, void* aos, cudaStream_t st);
+// the same seeded fields restricted to a t-slab of a global lattice of time
+// extent lt_glob: the links of slices t_first .. t_first + g.Lt - 1 (modulo
+// lt_glob) and one full spinor of the slab starting at slice t0
+cudaError_t launch_gauge_random_slab(const Geom& g, int lt_glob, int t_first, uint64_t seed, double eps, void* aos,
+                                     cudaStream_t st);
+cudaError_t launch_spinor_random_slab(const Geom& g, int lt_glob, int t0, uint64_t seed, void* aos, cudaStream_t st);
+int ingest_gauge(qcu_context ctx, const void* gauge);
+// slab contexts (comm.cu): the gauge field of the slab (local AoS), or the
+// seeded field of the global lattice restricted to the slab
+int dd_ingest_gauge(qcu_context ctx, const void* gauge);
+int dd_generate_gauge(qcu_context ctx, uint64_t seed, double eps);
 cudaError_t launch_clover_build(const Geom& g, const void* gauge64, double csw_eff, void* A64, void* Ainv64,
                                 void* Ainv32, void* Ainv16, int* status, cudaStream_t stream);
 cudaError_t launch_clover_apply(int prec, const Geom& g, int parity, int nrhs, CSpinorView in, SpinorView out,

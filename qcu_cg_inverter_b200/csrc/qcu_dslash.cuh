@@ -159,11 +159,11 @@ QCU_D void hop_dir(Spinor<R>& o, const Geom& g, const Nbrs& nb, int parity, int 
   Half2<R> h;
   // forward: U_mu(x) in(x+mu)
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  load_project<PS, MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t : R(1));
+  load_project<PS, MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.tf) ? bc_t : R(1));
   mul_reconstruct<MU, true, F, ROWS>(o, U, h);
   // backward: U_mu(x-mu)^dag in(x-mu); the link lives on the other parity
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  load_project<PS, MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t : R(1));
+  load_project<PS, MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.tb) ? bc_t : R(1));
   mul_reconstruct<MU, false, F, ROWS>(o, U, h);
 }
 
@@ -331,10 +331,10 @@ QCU_D void hop_dir_pair(SpinPair& o, const Geom& g, const Nbrs& nb, int parity, 
   HalfPair h;
   constexpr float unit = link_unit<PL>();
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.t == g.Lt - 1) ? bc_t * unit : unit);
+  float sc = load_project_pair<MU, true, F>(h, in, nb.fwd[MU], r, (MU == 3 && nb.tf) ? bc_t * unit : unit);
   mul_reconstruct_pair<MU, true, F>(o, U, h, sc);
   LinkIO<PL>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.t == 0) ? bc_t * unit : unit);
+  sc = load_project_pair<MU, false, F>(h, in, nb.bwd[MU], r, (MU == 3 && nb.tb) ? bc_t * unit : unit);
   mul_reconstruct_pair<MU, false, F>(o, U, h, sc);
 }
 

@@ -64,6 +64,15 @@ struct SolverWorkspace {
 };
 
 
+// Algorithmic bytes per site and RHS of the solver's passes (the counting of
+// qcuBenchStencil: every neighbour load, link and clover bytes divided by the
+// `share` RHS that one load serves): one sloppy iteration of operator variant
+// `op` (the four stencils and p = r + beta p), one reliable update, and the
+// admission plus retirement of a column.
+double iteration_bytes(int op, bool clover, int share);
+double reliable_update_bytes(int op, bool clover, int share);
+double admit_retire_bytes(bool clover, int share);
+
 struct OpCtx {
   qcu_context ctx;
   SolverWorkspace* w;

@@ -346,6 +346,7 @@ int qcuServerSubmit(qcu_server s, int config_id, double kappa, double csw, int n
 }
 
 int qcuServerPoll(qcu_server s, int* finished) {
+  NvtxRange nv("qcuServerPoll");
   clear_error();
   if (!s) {
     set_error(QCU_ERR_INVALID_ARG, "null server");

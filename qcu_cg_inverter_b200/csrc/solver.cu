@@ -91,6 +91,40 @@ __global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P
 #undef IV
 }
 
+static double sb_of(int prec) { return prec == PREC_DOUBLE ? 192.0 : (prec == PREC_SINGLE ? 96.0 : 52.0); }
+static double lb_of(int fmt) {
+  return fmt == PREC_DOUBLE ? 96.0 : (fmt == PREC_SINGLE ? 48.0 : (fmt == PREC_HALF ? 24.0 : 72.0));
+}
+static double cb_of(int prec) { return prec == PREC_DOUBLE ? 576.0 : (prec == PREC_SINGLE ? 288.0 : 148.0); }
+
+double iteration_bytes(int op, bool clover, int share) {
+  const double sb = sb_of(op_spinor_prec(op)), sa = sb_of(acc_prec(op_spinor_prec(op)));
+  const double lb = lb_of(op_link_format(op)), cb = clover ? cb_of(op_clover_prec(op)) : 0.0;
+  const double hop = 8.0 * sb + 8.0 * lb / share;
+  const double k1 = hop + cb / share + sb;             // t = A^-1 D p
+  const double k2 = hop + cb / share + 3.0 * sb;       // y, u from t and p
+  const double k3 = k1;                                 // t = A^-1 D^dag u
+  const double k4 = hop + 2.0 * sb + 4.0 * sa;          // z = y + c D^dag t, x and r updated
+  const double k5 = sa + 2.0 * sb;                      // p = r + beta p
+  return k1 + k2 + k3 + k4 + k5;
+}
+
+double reliable_update_bytes(int op, bool clover, int share) {
+  const double s64 = 192.0, l64 = 96.0, c64 = clover ? 576.0 : 0.0;
+  const double hop64 = 8.0 * s64 + 8.0 * l64 / share;
+  const double acc = sb_of(acc_prec(op_spinor_prec(op))) + 4.0 * s64;  // x_hi += x_lo, y = bhat - x_hi
+  const double res = 2.0 * hop64 + 2.0 * c64 / share + 3.0 * s64;      // r = bhat - Mhat x_hi
+  const double cres = s64 + 2.0 * c64 / share + 2.0 * sb_of(op_spinor_prec(op));
+  const double ne = iteration_bytes(op, clover, share) * 0.5;           // r_ne = Mhat^dag r, sloppy
+  return acc + res + cres + ne;
+}
+
+double admit_retire_bytes(bool clover, int share) {
+  const double s64 = 192.0, hop64 = 8.0 * s64 + 8.0 * 96.0 / share, c64 = clover ? 576.0 / share : 0.0;
+  // in: AoS -> internal (both parities), |b|^2, bhat; out: x_o, both parities to AoS
+  return 4.0 * s64 + 2.0 * s64 + (hop64 + c64 + 2.0 * s64) + s64 + (hop64 + c64 + 2.0 * s64) + 4.0 * s64;
+}
+
 int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover, double align) {
   cudaStream_t st = ctx->stream;
   const int pa = acc_prec(ps);
@@ -156,9 +190,37 @@ DslashArgs op_args(const OpCtx& o, int prec, int parity, const Field& in, const 
 }
 
 int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& a) {
-  QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, fin, a, o.w->shape, o.st));
+  if (!o.ctx->g.tdd) {
+    QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, fin, a, o.w->shape, o.st));
+    o.ctx->launches++;
+    return QCU_SUCCESS;
+  }
+  // a t-slab: the input's ghost slices from the neighbouring ranks first; the
+  // per-RHS sums of the launch are this slab's part, summed over the ranks
+  // before the finishing functor runs
+  QCU_CHECK(dd_exchange(o.ctx, a.in, op_spinor_prec(prec), o.st));
+  QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, FIN_NONE, a, o.w->shape, o.st));
   o.ctx->launches++;
+  if (epi & (EPI_NORM | EPI_CGXR)) {
+    QCU_CHECK(dd_sum(o.ctx, a.red.result, a.nrhs, o.st));
+    if (fin != FIN_NONE) {
+      QCU_CHECK_CUDA(launch_fin(fin, a.red, a.nrhs, o.st));
+      o.ctx->launches++;
+    }
+  }
   return QCU_SUCCESS;
+}
+
+template <class Fin>
+__global__ void fin_kernel(const ReduceArgs red, int nrhs) {
+  Fin::apply(red.result, nrhs, 1, red.state);
+}
+
+cudaError_t launch_fin(int fin, const ReduceArgs& red, int nrhs, cudaStream_t st) {
+  if (fin == FIN_CG_ALPHA) fin_kernel<FinCgAlpha><<<1, 1, 0, st>>>(red, nrhs);
+  else if (fin == FIN_CG_BETA) fin_kernel<FinCgBeta><<<1, 1, 0, st>>>(red, nrhs);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
 }
 
 ReduceArgs red_into(const OpCtx& o, double* result, bool with_state) {
@@ -262,6 +324,7 @@ int reliable_update(const OpCtx& o, bool fresh) {
                                      ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
                                      w.di(I_CIDX), upd, red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
     o.ctx->launches++;
+    QCU_CHECK(dd_sum(o.ctx, w.dd(D_RES_AR2), w.nrhs, o.st));
   } else if (sloppy_ne) {
     QCU_CHECK_CUDA(launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.y.view(0), w.y64.cview(0), upd, nullptr, w.shape, o.st));
     o.ctx->launches++;

@@ -19,6 +19,8 @@ def declared_functions():
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", src, flags=re.M):
             name = m.group(1)
+            if m.group(0).lstrip().startswith("typedef"):  # function-pointer types, not functions
+                continue
             if name not in ("typedef", "struct"):
                 names.append(name)
     return sorted(set(names))

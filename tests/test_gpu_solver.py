@@ -198,3 +198,24 @@ def test_repeated_solves_reuse_the_first_solves_step_plan(cuda, qcu_lib, oracle)
             counts.append(c.launches - n0)
         assert counts[1] == counts[2], counts
         assert counts[1] <= 1.1 * counts[0], counts
+
+
+def test_solve_report_carries_time_and_bytes(cuda, qcu_lib, oracle):
+    """Every report of a qcuInvert call carries the call's device time and
+    GB/s and the RHS's own algorithmic bytes (positive, and growing with the
+    iterations it took)."""
+    L = (8, 8, 8, 8)
+    U = oracle.gauge_random(L, 5, 0.4)
+    bs = np.stack([oracle.full_spinor_random(L, 30 + r) for r in range(3)])
+    with qcu_lib.Context(L) as c:
+        c.load_gauge(dev(U))
+        xb = dev(np.zeros_like(bs))
+        reps = c.invert(xb, dev(bs), nrhs=3, kappas=[0.125, 0.13, 0.1375], csw=1.0, tol=1e-10, precision="half")
+    secs = {r["seconds"] for r in reps}
+    assert len(secs) == 1 and secs.pop() > 0
+    total = sum(r["gbytes"] for r in reps)
+    assert all(r["gbytes"] > 0 for r in reps)
+    assert abs(reps[0]["gbytes_per_s"] * reps[0]["seconds"] - total) < 1e-9 * max(total, 1)
+    # more iterations, more bytes
+    order = sorted(reps, key=lambda r: r["iterations"])
+    assert order[0]["gbytes"] <= order[-1]["gbytes"]
