@@ -31,8 +31,10 @@ reference library is GPU-only; its host-side restatement is the oracle's FP64
 CG, run with every host thread) and adds the reference library's own Dslash
 kernels (its printed kernel times) and entry points timed on the GPU.
 
-Multi-GPU: the solve does not shard in this build (one lattice per GPU), so
-N ranks run N independent replicas; value = total solves / max-over-ranks time.
+Multi-GPU: by default N ranks run N independent replicas of the headline
+solve (weak scaling); value = total solves / max-over-ranks time. --dd
+instead splits one 32^3x64 lattice into N t-slabs (halo exchange and sums
+over NCCL; strong scaling).
 `--gpus N` outside torchrun relaunches this script under torchrun with N
 local ranks; under torchrun it must equal WORLD_SIZE.
 """
@@ -780,6 +782,53 @@ def run_stencil(args):
                       "frac": gbs / hbm, "peak_source": src}), flush=True)
 
 
+def run_dd(args, world, rank, local):
+    """One lattice decomposed along t over the N ranks (strong scaling): the
+    32^3x64 Wilson-clover solve of the large workload (kappa 0.1370, eps 0.5)
+    on SlabContexts, halo exchange and sums over NCCL (one rank: NCCL to
+    itself). Time per solve is the max over ranks of the CUDA-event time."""
+    import torch
+    import torch.distributed as dist
+
+    import qcu_cg_inverter_b200 as q
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        comm = q.Comm.torch_distributed(local)
+    else:
+        comm = q.Comm.nccl(q.Comm.nccl_unique_id(), 1, 0, local)
+    s = q.SlabContext(ROOF_LATTICE, comm, local)
+    s.generate_gauge(GAUGE_SEED, LARGE_EPS)
+    s.set_half_operator(STORAGE[args.storage])
+    vh = s.volume // 2
+    b = torch.empty(2 * vh * 12, dtype=torch.complex128, device=device)
+    s.generate_spinor(b, 1, SOURCE_SEED)
+    x = torch.zeros_like(b)
+    stream = torch.cuda.ExternalStream(s.stream, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    kw = dict(kappa=LARGE_KAPPA, csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta, precision=args.precision)
+    for _ in range(max(args.warmup, 1)):
+        rep = s.invert(x, b, **kw)[0]
+    barrier(world, device)
+    steps = max(1, min(args.steps, 5))
+    t, rep = timed_steps(torch, device, stream, flush, lambda: s.invert(x, b, **kw)[0], steps)
+    t = max_over_ranks(t, world, device)
+    storage = s.half_storage(1)
+    s.close()  # its CUDA graphs hold NCCL calls: released before the communicator
+    comm.close()
+    if rank != 0:
+        return None
+    return {"metric": "CG time to |r|/|b|<1e-10, one 32^3x64 lattice decomposed along t", "value": steps / t,
+            "unit": "solves/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": t / steps * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": DTYPE[storage], "data": "synthetic",
+            "config": {"workload": "32^3x64 Wilson-clover, t-slabs", "lattice": ROOF_LATTICE, "kappa": LARGE_KAPPA,
+                       "csw": CSW, "eps": LARGE_EPS, "parallelism": f"t-slabs x{world}",
+                       "transport": "nccl" if world == 1 or dist.get_backend() == "nccl" else "host"},
+            "iterations": rep["iterations"], "reliable_updates": rep["reliable_updates"],
+            "true_residual": rep["true_residual"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -801,6 +850,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the large solve, the 48-RHS batch and the serving stream in the default line")
+    ap.add_argument("--dd", action="store_true",
+                    help="one 32^3x64 lattice decomposed along t over the --gpus ranks (strong scaling)")
     ap.add_argument("--plan", action="store_true",
                     help="print the rank layout each process sees (after any --gpus relaunch) and exit")
     ap.add_argument("--oracle-check", action="store_true", help="--multi: recompute each residual with the oracle")
@@ -833,7 +884,9 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    if args.impl == "reference":
+    if args.dd:
+        out = run_dd(args, world, rank, local)
+    elif args.impl == "reference":
         out = run_reference(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
