@@ -83,18 +83,17 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
     return cudaErrorInvalidConfiguration;
   dim3 block(tx, sh.Sb);
   const int nslab = (a.nrhs + sh.Rb - 1) / sh.Rb;
-  // the RHS-paired kernels with staged hops take two shared-memory slots per thread
-  const size_t smem = (per_thread == 2 && QCU_PAIR_STAGE) ? pair_stage_bytes(tx * sh.Sb) : 0;
+
   if (QCU_SLAB_MINOR && nslab > 1) {
     // the RHS tiles of one site tile run back to back, so its links and
     // clover are read from DRAM once and served from L2 to the others
     DslashArgs b = a;
     b.nslab = nslab;
-    fn<<<dim3(grid_x(a.g.Vh, sh.Sb) * nslab, 1), block, smem, stream>>>(b);
+    fn<<<dim3(grid_x(a.g.Vh, sh.Sb) * nslab, 1), block, 0, stream>>>(b);
   } else {
     DslashArgs b = a;
     b.nslab = 0;
-    fn<<<dim3(grid_x(a.g.Vh, sh.Sb), nslab), block, smem, stream>>>(b);
+    fn<<<dim3(grid_x(a.g.Vh, sh.Sb), nslab), block, 0, stream>>>(b);
   }
   return cudaGetLastError();
 }

@@ -180,148 +180,6 @@ QCU_D void hop_rp(PairSpinor& o, const Geom& g, int parity, int s, RhsPair rp, c
   hop_dir_rp<3, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
 }
 
-// ---------------------------------------------------------------------------
-// Staged hop: each thread copies the next hop's link and neighbour words into
-// its own slot of shared memory with asynchronous copies (cp.async, sm_80+:
-// the data travels without occupying registers) while it computes the current
-// hop from the slot filled before, so one hop's loads are always in flight
-// behind the arithmetic. Two slots per thread; the slots are private, so the
-// only wait is the thread's own cp.async.wait_group. Same arithmetic as hop_rp.
-// ---------------------------------------------------------------------------
-struct PairSlot {
-  int4 w0[3], w1[3];  // the lanes' 16-bit chunks of the neighbour spinor
-  float2 nm;          // the lanes' norms
-  float2 pad;
-  float4 lk[5];       // the link, 18 FP32 reals in 5 chunks
-};
-static_assert(sizeof(PairSlot) == kPairSlotBytes, "slot layout");
-
-QCU_D void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-QCU_D void cp_async4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-QCU_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// waits until at most N of this thread's committed groups are pending
-template <int N> QCU_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// hop h = 2*MU + (FWD ? 0 : 1): its link and neighbour into slot `sl`
-template <int MU, bool FWD>
-QCU_D void pair_issue(PairSlot* sl, const Geom& g, const Nbrs& nb, int parity, int s, RhsPair rp,
-                      const CSpinorView& in, const void* gauge) {
-  const int sn = FWD ? nb.fwd[MU] : nb.bwd[MU];
-  const int ls = FWD ? s : sn;
-  const int lpar = FWD ? parity : 1 - parity;
-  const float4* L = static_cast<const float4*>(gauge) + (size_t)(MU * 2 + lpar) * g.Vh_pad * 5;
-  const unsigned l0 = (unsigned)chunk_index(0, ls, 0, 5, 1);
-#pragma unroll
-  for (int c = 0; c < 5; c++) cp_async16(&sl->lk[c], L + l0 + 32u * c);
-  const int4* p = static_cast<const int4*>(in.data);
-  const unsigned i0 = (unsigned)chunk_index(0, sn, rp.r0, 3, in.nrhs);
-  const unsigned cs = 32u * (unsigned)in.nrhs;
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    cp_async16(&sl->w0[c], p + i0 + c * cs);
-    cp_async16(&sl->w1[c], p + i0 + c * cs + rp.d);
-  }
-  const unsigned n0 = (unsigned)site_rhs_index(sn, rp.r0, in.nrhs);
-  cp_async4(&sl->nm.x, in.norm + n0);
-  cp_async4(&sl->nm.y, in.norm + n0 + rp.d);
-}
-
-// hop h from its slot (the projection and reconstruction of hop_dir_rp)
-template <int MU, bool FWD, int F>
-QCU_D void pair_consume(PairSpinor& o, const PairSlot* sl, float phase) {
-  constexpr int S = FWD ? -F : F;
-  constexpr float fS = (float)S;
-  Link<float> U;
-  {
-    float4 w[5];
-#pragma unroll
-    for (int c = 0; c < 5; c++) w[c] = sl->lk[c];
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      U.u[2 * c] = mk(w[c].x, w[c].y);
-      U.u[2 * c + 1] = mk(w[c].z, w[c].w);
-    }
-    U.u[8] = mk(w[4].x, w[4].y);
-  }
-  int4 w0[3], w1[3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    w0[c] = sl->w0[c];
-    w1[c] = sl->w1[c];
-  }
-  const float2 sc = fmul2(sl->nm, splat2(kInvFix * phase));
-  float2 h0re[3], h0im[3], h1re[3], h1im[3];
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    float2 pre[4], pim[4];
-#pragma unroll
-    for (int sp = 0; sp < 4; sp++) {
-      const int a = word_of(w0, 3 * sp + c), b = word_of(w1, 3 * sp + c);
-      pre[sp] = dec_lo2(a, b);
-      pim[sp] = dec_hi2(a, b);
-    }
-    if constexpr (MU == 0) {
-      h0re[c] = ffma2(pim[3], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pre[3], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pim[2], splat2(-fS), pre[1]);
-      h1im[c] = ffma2(pre[2], splat2(fS), pim[1]);
-    } else if constexpr (MU == 1) {
-      h0re[c] = ffma2(pre[3], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pim[3], splat2(-fS), pim[0]);
-      h1re[c] = ffma2(pre[2], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pim[2], splat2(fS), pim[1]);
-    } else if constexpr (MU == 2) {
-      h0re[c] = ffma2(pim[2], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pre[2], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pim[3], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pre[3], splat2(-fS), pim[1]);
-    } else {
-      h0re[c] = ffma2(pre[2], splat2(fS), pre[0]);
-      h0im[c] = ffma2(pim[2], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pre[3], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pim[3], splat2(fS), pim[1]);
-    }
-  }
-  mul_reconstruct_rp<MU, FWD, F>(o, U, h0re, h0im, h1re, h1im, sc);
-}
-
-// hop_rp with the loads staged through the thread's two slots (slots[0..1])
-template <bool DAG>
-QCU_D void hop_rp_staged(PairSpinor& o, PairSlot* slots, const Geom& g, int parity, int s, RhsPair rp,
-                         const CSpinorView& in, const void* gauge, float bc_t) {
-  constexpr int F = DAG ? -1 : 1;
-#pragma unroll
-  for (int k = 0; k < 12; k++) o.re[k] = o.im[k] = make_float2(0.f, 0.f);
-  const Nbrs nb = neighbours(g, s, parity);
-  const float ph_f = nb.tf ? bc_t : 1.f, ph_b = nb.tb ? bc_t : 1.f;
-  pair_issue<0, true>(slots + 0, g, nb, parity, s, rp, in, gauge);
-  cp_async_commit();
-  pair_issue<0, false>(slots + 1, g, nb, parity, s, rp, in, gauge);
-  cp_async_commit();
-  // hop h is in slot h % 2; after consuming it, the slot takes hop h + 2
-#define QCU_PAIR_STEP(MU, FWD, NMU, NFWD, LAST)                                   \
-  cp_async_wait<1>();                                                             \
-  pair_consume<MU, FWD, F>(o, slots + ((2 * MU + (FWD ? 0 : 1)) & 1),           \
-                           MU == 3 ? (FWD ? ph_f : ph_b) : 1.f);                  \
-  if (!LAST) pair_issue<NMU, NFWD>(slots + ((2 * MU + (FWD ? 0 : 1)) & 1), g, nb, parity, s, rp, in, gauge); \
-  cp_async_commit();
-  QCU_PAIR_STEP(0, true, 1, true, false)
-  QCU_PAIR_STEP(0, false, 1, false, false)
-  QCU_PAIR_STEP(1, true, 2, true, false)
-  QCU_PAIR_STEP(1, false, 2, false, false)
-  QCU_PAIR_STEP(2, true, 3, true, false)
-  QCU_PAIR_STEP(2, false, 3, false, false)
-  QCU_PAIR_STEP(3, true, 3, true, true)
-  QCU_PAIR_STEP(3, false, 3, false, true)
-#undef QCU_PAIR_STEP
-}
-
 // Element pair of the block-interleaved FP32 clover: chunk q of the lanes'
 // fields holds (b0[2q], b1[2q], b0[2q+1], b1[2q+1]); E = element 2q + h of
 // block b is float b + 2h of the chunk. UNI: both lanes read one field, so the
@@ -528,14 +386,7 @@ QCU_D void dslash_pair_body(const DslashArgs& a) {
   if (v0 || v1) {
     const int r1 = r0 + rp.d;
     PairSpinor o;
-    if constexpr (QCU_PAIR_STAGE != 0) {
-      extern __shared__ __align__(16) unsigned char qcu_dyn_smem[];
-      PairSlot* slots = reinterpret_cast<PairSlot*>(qcu_dyn_smem) +
-                        (size_t)kPairSlots * (threadIdx.y * blockDim.x + threadIdx.x);
-      hop_rp_staged<DAG>(o, slots, a.g, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
-    } else {
-      hop_rp<DAG>(o, a.g, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
-    }
+    hop_rp<DAG>(o, a.g, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
     const bool need_clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) != 0;
     const void* c0 = need_clov ? clover_of(a, r0) : nullptr;
     const void* c1 = need_clov ? clover_of(a, r1) : nullptr;

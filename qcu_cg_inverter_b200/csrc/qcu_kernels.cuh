@@ -72,16 +72,6 @@ cudaError_t launch_dslash(int op, bool dagger, int epi, int fin, const DslashArg
 // kernels for every epilogue (1), on one RHS per thread (0), or as built (-1).
 void set_rhs_pairs_override(int v);
 
-// RHS-paired kernels: hops staged through shared memory (1) or loaded straight
-// into registers (0); with staging each thread holds kPairSlots slots of
-// kPairSlotBytes (its next hop's link and neighbour words) in dynamic shared memory.
-#ifndef QCU_PAIR_STAGE
-#define QCU_PAIR_STAGE 0
-#endif
-constexpr int kPairSlots = 2;
-constexpr size_t kPairSlotBytes = 192;
-inline size_t pair_stage_bytes(int nthreads) { return (size_t)kPairSlots * nthreads * kPairSlotBytes; }
-
 // Number of blocks along x for a field of Vh sites.
 inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }
 
