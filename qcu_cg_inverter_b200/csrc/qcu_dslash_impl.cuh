@@ -58,6 +58,12 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #define QCU_DSLASH_MINB_PAIR_OUT2 QCU_DSLASH_MINB_PAIR
 #endif
 constexpr int dslash_maxt(int op) { return op == OP_HALF_FAST_2 ? 128 : 256; }
+// the compact single-RHS family (OP_HALF_1): 128 registers. Measured at
+// 32^3x64 against the 85-register cap (80 used, 28 B spilled): K2 170 vs 164
+// us, K4 134 vs 136 us, the solve 29.1 vs 29.2 ms - even, so no cap
+#ifndef QCU_DSLASH_MINB_C1
+#define QCU_DSLASH_MINB_C1 QCU_DSLASH_MINB
+#endif
 // batched FP64 launches (reliable updates of multi-RHS solves): the
 // 128-register cap with row-at-a-time reconstruction (measured in the 48-RHS
 // 24^3x48 solve: 0.556 vs 0.568 s)
@@ -65,7 +71,8 @@ constexpr int dslash_maxt(int op) { return op == OP_HALF_FAST_2 ? 128 : 256; }
 #define QCU_DSLASH_MINB64_BATCH 2
 #endif
 constexpr int dslash_minb(int op, int epi) {
-  return op == OP_DOUBLE ? QCU_DSLASH_MINB64
+  return op == OP_HALF_1 ? QCU_DSLASH_MINB_C1
+         : op == OP_DOUBLE ? QCU_DSLASH_MINB64
          : op == OP_DOUBLE_BATCH ? QCU_DSLASH_MINB64_BATCH
          : op == OP_HALF_FAST_2 ? ((epi & EPI_OUT2) ? QCU_DSLASH_MINB_PAIR_OUT2 : QCU_DSLASH_MINB_PAIR)
          : (op_spinor_prec(op) != PREC_HALF || ((op == OP_HALF_FAST_1 || op == OP_HALF_1) && !QCU_DSLASH_CAP_1RHS))
