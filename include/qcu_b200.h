@@ -109,7 +109,12 @@ void qcuSolveParamsDefault(qcu_solve_params* params);
 int qcuContextCreate(qcu_context* ctx, const int lattice[4], int device);
 int qcuContextDestroy(qcu_context ctx);
 /* Orders the context's own stream after the caller's stream (cudaStream_t):
- * work enqueued later by the context starts after what `stream` holds now. */
+ * work enqueued later by the context starts after what `stream` holds now.
+ * The context's stream does not wait for any other stream by itself, so a
+ * caller whose arguments come from kernels still pending on its own stream
+ * calls this first (the Python binding does it for torch tensors, with
+ * torch's current stream); the reference-interface entry points (qcu.h) order
+ * themselves after the default stream, as the reference's calls ran on it. */
 int qcuContextSetStream(qcu_context ctx, void* stream);
 /* The context's own stream (cudaStream_t), for recording events around calls. */
 void* qcuContextGetStream(qcu_context ctx);

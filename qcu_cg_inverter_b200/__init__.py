@@ -382,30 +382,49 @@ class Context:
         L = self.lattice
         return L[0] * L[1] * L[2] * L[3]
 
+    def _after_torch(self, *fields):
+        """Orders the context's stream after torch's current stream when a
+        field is a CUDA tensor: the kernels that produced it, or that still
+        read an output buffer, may be pending there (the library's stream
+        does not wait for the default stream by itself)."""
+        for x in fields:
+            if getattr(x, "is_cuda", False):
+                import torch
+                s = torch.cuda.current_stream(x.device)
+                _check(lib().qcuContextSetStream(self._h, ctypes.c_void_p(s.cuda_stream)))
+                return
+
     def load_gauge(self, gauge):
+        self._after_torch(gauge)
         _check(lib().qcuLoadGauge(self._h, _ptr(gauge)))
 
     def generate_gauge(self, seed: int, eps: float):
         _check(lib().qcuGenerateGauge(self._h, int(seed), float(eps)))
 
     def export_gauge(self, out):
+        self._after_torch(out)
         _check(lib().qcuExportGauge(self._h, _ptr(out)))
 
     def generate_spinor(self, out, nrhs: int, seed: int):
+        self._after_torch(out)
         _check(lib().qcuGenerateSpinor(self._h, _ptr(out), int(nrhs), int(seed)))
 
     def dslash(self, out, inp, parity: int, dagger: int = 0, bc_t: float = 1.0):
+        self._after_torch(inp, out)
         _check(lib().qcuDslash(self._h, _ptr(out), _ptr(inp), int(parity), int(dagger), float(bc_t)))
 
     def apply_clover(self, out, inp, csw_eff: float, inverse: bool):
+        self._after_torch(inp, out)
         _check(lib().qcuApplyClover(self._h, _ptr(out), _ptr(inp), float(csw_eff), int(bool(inverse))))
 
     def apply_operator(self, out, inp, kappa: float, csw: float, bc_t: float = -1.0, dagger: int = 0):
+        self._after_torch(inp, out)
         _check(lib().qcuApplyOperator(self._h, _ptr(out), _ptr(inp), float(kappa), float(csw), float(bc_t),
                                       int(dagger)))
 
     def invert(self, x, b, nrhs: int = 1, kappas=None, raise_on_fail: bool = True, **kw):
         sp = solve_params(**kw)
+        self._after_torch(b, x)
         reps = (SolveReport * nrhs)()
         karr = None
         if kappas is not None:

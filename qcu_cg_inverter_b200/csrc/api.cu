@@ -330,7 +330,11 @@ static DslashArgs base_args(qcu_context ctx, int prec) {
 }
 
 static int run_dslash(qcu_context ctx, int prec, bool dag, int epi, const DslashArgs& a) {
-  QCU_CHECK(dd_exchange(ctx, a.in, op_spinor_prec(prec), ctx->stream));  // t-slab: the neighbours' faces
+  if (ctx->g.tdd)  // t-slab: the neighbours' faces, beside the interior
+    return dd_stencil(ctx, a, op_spinor_prec(prec), ctx->shape1, ctx->stream, [&](const DslashArgs& piece) {
+      ctx->launches++;
+      return launch_dslash(prec, dag, epi, FIN_NONE, piece, ctx->shape1, ctx->stream);
+    });
   QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, FIN_NONE, a, ctx->shape1, ctx->stream));
   ctx->launches++;
   return QCU_SUCCESS;
@@ -439,6 +443,9 @@ static int legacy_begin(QcuParam* param, void* gauge, qcu_context* out) {
       }
   }
   QCU_CHECK(ctx_check(g_legacy));
+  // the reference works on the default stream: the caller's pending work on
+  // it (the kernels that produced the arguments) comes first
+  QCU_CHECK(qcuContextSetStream(g_legacy, cudaStreamLegacy));
   if (gauge && (!g_legacy->gauge_loaded || g_legacy->legacy_gauge_src != gauge)) {
     QCU_CHECK(ingest_gauge(g_legacy, gauge));
     g_legacy->legacy_gauge_src = gauge;
@@ -524,6 +531,12 @@ int qcuContextDestroy(qcu_context ctx) {
   cudaStreamSynchronize(ctx->stream);
   qcu_solver_workspace_free(ctx);
   if (ctx->ext) qcuContextDestroy(ctx->ext);
+  if (ctx->dd_stream) {
+    cudaStreamSynchronize(ctx->dd_stream);
+    cudaStreamDestroy(ctx->dd_stream);
+  }
+  for (cudaEvent_t e : ctx->dd_ev)
+    if (e) cudaEventDestroy(e);
   delete ctx;
   return QCU_SUCCESS;
 }

@@ -108,8 +108,40 @@ static int nccl_status(ncclResult_t r, const char* what) {
     if (_r != ncclSuccess) return ::qcu::nccl_status(_r, #expr); \
   } while (0)
 
-// send_lo -> rank-1 (its recv_hi), send_hi -> rank+1 (its recv_lo); device
-// pointers, enqueued on st
+// One contiguous piece of a face exchange: send_lo -> rank-1 (its recv_hi),
+// send_hi -> rank+1 (its recv_lo); device pointers.
+struct FaceSeg {
+  const void *send_lo, *send_hi;
+  void *recv_lo, *recv_hi;
+  size_t bytes;
+};
+
+static int comm_exchange(qcu_comm c, const void* send_lo, const void* send_hi, void* recv_lo, void* recv_hi,
+                         size_t bytes, cudaStream_t st);
+
+// Several pieces in one exchange (a 16-bit field's words and norms): one NCCL
+// group, so the transfers of all pieces go together
+static int comm_exchange_segs(qcu_comm c, const FaceSeg* seg, int n, cudaStream_t st) {
+  if (c->host) {
+    for (int i = 0; i < n; i++)
+      QCU_CHECK(comm_exchange(c, seg[i].send_lo, seg[i].send_hi, seg[i].recv_lo, seg[i].recv_hi, seg[i].bytes, st));
+    return QCU_SUCCESS;
+  }
+  const int lo = (c->rank + c->nranks - 1) % c->nranks, hi = (c->rank + 1) % c->nranks;
+  // the same order on every rank: with two ranks lo == hi and the pairs match
+  // in issue order (my send_lo with the peer's recv_hi); one rank sends to itself
+  QCU_CHECK_NCCL(g_nccl.GroupStart());
+  for (int i = 0; i < n; i++) {
+    if (!seg[i].bytes) continue;
+    QCU_CHECK_NCCL(g_nccl.Send(seg[i].send_lo, seg[i].bytes, ncclChar, lo, c->nccl, st));
+    QCU_CHECK_NCCL(g_nccl.Recv(seg[i].recv_hi, seg[i].bytes, ncclChar, hi, c->nccl, st));
+    QCU_CHECK_NCCL(g_nccl.Send(seg[i].send_hi, seg[i].bytes, ncclChar, hi, c->nccl, st));
+    QCU_CHECK_NCCL(g_nccl.Recv(seg[i].recv_lo, seg[i].bytes, ncclChar, lo, c->nccl, st));
+  }
+  QCU_CHECK_NCCL(g_nccl.GroupEnd());
+  return QCU_SUCCESS;
+}
+
 static int comm_exchange(qcu_comm c, const void* send_lo, const void* send_hi, void* recv_lo, void* recv_hi,
                          size_t bytes, cudaStream_t st) {
   if (bytes == 0) return QCU_SUCCESS;
@@ -118,18 +150,9 @@ static int comm_exchange(qcu_comm c, const void* send_lo, const void* send_hi, v
     QCU_CHECK_CUDA(cudaMemcpyAsync(recv_lo, send_hi, bytes, cudaMemcpyDeviceToDevice, st));
     return QCU_SUCCESS;
   }
-  const int lo = (c->rank + c->nranks - 1) % c->nranks, hi = (c->rank + 1) % c->nranks;
   if (!c->host) {
-    // the same order on every rank: with two ranks lo == hi and the pairs
-    // match in issue order (my send_lo with the peer's recv_hi); one rank
-    // sends to itself
-    QCU_CHECK_NCCL(g_nccl.GroupStart());
-    QCU_CHECK_NCCL(g_nccl.Send(send_lo, bytes, ncclChar, lo, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Recv(recv_hi, bytes, ncclChar, hi, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Send(send_hi, bytes, ncclChar, hi, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Recv(recv_lo, bytes, ncclChar, lo, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.GroupEnd());
-    return QCU_SUCCESS;
+    const FaceSeg s{send_lo, send_hi, recv_lo, recv_hi, bytes};
+    return comm_exchange_segs(c, &s, 1, st);
   }
   for (PinnedBuf* b : {&c->hsend_lo, &c->hsend_hi, &c->hrecv_lo, &c->hrecv_hi}) QCU_CHECK(b->ensure(bytes));
   QCU_CHECK_CUDA(cudaMemcpyAsync(c->hsend_lo.p, send_lo, bytes, cudaMemcpyDeviceToHost, st));
@@ -173,12 +196,64 @@ int dd_exchange(qcu_context ctx, const CSpinorView& v, int prec, cudaStream_t st
   const size_t f = (size_t)g.st;  // sites of a slice
   const size_t per = chunk_bytes_per_site(prec) * v.nrhs;
   char* d = const_cast<char*>(static_cast<const char*>(v.data));
-  QCU_CHECK(comm_exchange(ctx->comm, d, d + (g.Vh - f) * per, d + g.gbwd * per, d + g.gfwd * per, f * per, st));
+  FaceSeg seg[2];
+  int n = 0;
+  seg[n++] = FaceSeg{d, d + (g.Vh - f) * per, d + g.gbwd * per, d + g.gfwd * per, f * per};
   if (prec == PREC_HALF) {
     const size_t pn = sizeof(float) * v.nrhs;
-    char* n = const_cast<char*>(reinterpret_cast<const char*>(v.norm));
-    QCU_CHECK(comm_exchange(ctx->comm, n, n + (g.Vh - f) * pn, n + g.gbwd * pn, n + g.gfwd * pn, f * pn, st));
+    char* m = const_cast<char*>(reinterpret_cast<const char*>(v.norm));
+    seg[n++] = FaceSeg{m, m + (g.Vh - f) * pn, m + g.gbwd * pn, m + g.gfwd * pn, f * pn};
   }
+  if (ctx->comm->host && ctx->comm->nranks == 1) {
+    for (int i = 0; i < n; i++)
+      QCU_CHECK(comm_exchange(ctx->comm, seg[i].send_lo, seg[i].send_hi, seg[i].recv_lo, seg[i].recv_hi, seg[i].bytes,
+                              st));
+    return QCU_SUCCESS;
+  }
+  return comm_exchange_segs(ctx->comm, seg, n, st);
+}
+
+// the interior of a slab stencil beside the face exchange (1), or the
+// exchange first and then the whole slab (0)
+#ifndef QCU_DD_OVERLAP
+#define QCU_DD_OVERLAP 1
+#endif
+
+int dd_stencil(qcu_context ctx, const DslashArgs& a, int prec, LaunchShape sh, cudaStream_t st,
+               const std::function<cudaError_t(const DslashArgs&)>& launch) {
+  if (!QCU_DD_OVERLAP) {
+    QCU_CHECK(dd_exchange(ctx, a.in, prec, st));
+    QCU_CHECK_CUDA(launch(a));
+    return QCU_SUCCESS;
+  }
+  const Geom& g = ctx->g;
+  const int f = g.st;
+  const int rt = (a.nrhs + sh.Rb - 1) / sh.Rb;  // RHS tiles
+  // pieces: the interior slices, then the first and the last slice
+  const int lo[3] = {f, 0, g.Vh - f}, hi[3] = {g.Vh - f, f, g.Vh};
+  int tiles[3], total_tiles = 0;
+  for (int k = 0; k < 3; k++) {
+    tiles[k] = hi[k] > lo[k] ? (hi[k] - lo[k] + sh.Sb - 1) / sh.Sb : 0;
+    total_tiles += tiles[k];
+  }
+  DslashArgs p[3];
+  for (int k = 0, off = 0; k < 3; k++) {
+    p[k] = a;
+    p[k].s_off = lo[k];
+    p[k].s_lim = hi[k];
+    p[k].tile_off = off;
+    p[k].tile_total = total_tiles;
+    p[k].block_total = total_tiles * rt;
+    off += tiles[k];
+  }
+  QCU_CHECK_CUDA(cudaEventRecord(ctx->dd_ev[0], st));  // the input is complete
+  if (tiles[0]) QCU_CHECK_CUDA(launch(p[0]));        // the interior needs no ghost slice
+  QCU_CHECK_CUDA(cudaStreamWaitEvent(ctx->dd_stream, ctx->dd_ev[0], 0));
+  QCU_CHECK(dd_exchange(ctx, a.in, prec, ctx->dd_stream));
+  QCU_CHECK_CUDA(cudaEventRecord(ctx->dd_ev[1], ctx->dd_stream));
+  QCU_CHECK_CUDA(cudaStreamWaitEvent(st, ctx->dd_ev[1], 0));
+  for (int k = 1; k < 3; k++)
+    if (tiles[k]) QCU_CHECK_CUDA(launch(p[k]));
   return QCU_SUCCESS;
 }
 
@@ -410,6 +485,13 @@ extern "C" int qcuContextCreateSlab(qcu_context* out, const int lattice[4], qcu_
   ctx->g = make_geom_slab(lattice, comm->nranks, comm->rank);
   ctx->comm = comm;
   ctx->ext = ext;
+  if (cudaStreamCreateWithFlags(&ctx->dd_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->dd_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->dd_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    qcuContextDestroy(ctx);
+    return cuda_status(e, "slab exchange stream");
+  }
   ctx->Lt_global = lattice[3];
   ctx->t0 = geo[0];
   *out = ctx;

@@ -83,17 +83,19 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
     return cudaErrorInvalidConfiguration;
   dim3 block(tx, sh.Sb);
   const int nslab = (a.nrhs + sh.Rb - 1) / sh.Rb;
+  const int nsites = (a.s_lim > 0 ? a.s_lim : a.g.Vh) - a.s_off;
+  if (nsites <= 0) return cudaSuccess;
 
   if (QCU_SLAB_MINOR && nslab > 1) {
     // the RHS tiles of one site tile run back to back, so its links and
     // clover are read from DRAM once and served from L2 to the others
     DslashArgs b = a;
     b.nslab = nslab;
-    fn<<<dim3(grid_x(a.g.Vh, sh.Sb) * nslab, 1), block, 0, stream>>>(b);
+    fn<<<dim3(grid_x(nsites, sh.Sb) * nslab, 1), block, 0, stream>>>(b);
   } else {
     DslashArgs b = a;
     b.nslab = 0;
-    fn<<<dim3(grid_x(a.g.Vh, sh.Sb), nslab), block, 0, stream>>>(b);
+    fn<<<dim3(grid_x(nsites, sh.Sb), nslab), block, 0, stream>>>(b);
   }
   return cudaGetLastError();
 }

@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -156,6 +157,8 @@ struct qcu_context_s {
   qcu_comm comm = nullptr;
   int Lt_global = 0, t0 = 0;
   qcu_context ext = nullptr;
+  cudaStream_t dd_stream = nullptr;  // the halo exchange, beside the interior stencil
+  cudaEvent_t dd_ev[2] = {nullptr, nullptr};
   ~qcu_context_s();
 };
 
@@ -208,6 +211,12 @@ cudaError_t preload_spinor_io_f64();
 // (both no-ops on a context that is not a slab)
 int dd_exchange(qcu_context ctx, const CSpinorView& v, int prec, cudaStream_t st);
 int dd_sum(qcu_context ctx, double* values, int n, cudaStream_t st);
+// One stencil on a slab with the exchange of its input's faces overlapped:
+// `launch` enqueues a piece of the stencil (a over a site range) on st; the
+// interior slices run while the faces travel on the context's exchange
+// stream, then the first and last slices. The pieces share a's reduction.
+int dd_stencil(qcu_context ctx, const DslashArgs& a, int prec, LaunchShape sh, cudaStream_t st,
+               const std::function<cudaError_t(const DslashArgs&)>& launch);
 // copies the slab's part of the extended slab's clover slot into its own slot
 int dd_clover_from_ext(qcu_context ctx, int ext_slot, int slot);
 // the finishing functor `fin` (FinId) applied to reduced totals, as the

@@ -184,8 +184,8 @@ QCU_D void dslash_site_body(const DslashArgs& a) {
   typedef typename CompReal<PS>::type R;
   const TileCoord tc = stencil_tile(a);
   const int r = tc.rhs * blockDim.x + threadIdx.x;
-  const int s = tc.site * blockDim.y + threadIdx.y;
-  const bool valid = (s < a.g.Vh) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
+  const int s = stencil_site0(a, tc) + threadIdx.y;
+  const bool valid = (s < stencil_slim(a)) && (r < a.nrhs) && (a.active == nullptr || a.active[r]);
   double nrm = 0.0;
   // single-RHS launches of the fast 16-bit operator: block-paired epilogues
   // (measured: 16^3x32 solve 3.70 vs 3.88 ms); with many RHS per launch the

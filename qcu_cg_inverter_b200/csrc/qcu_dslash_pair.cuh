@@ -376,8 +376,8 @@ template <bool DAG, int EPI, class Fin>
 QCU_D void dslash_pair_body(const DslashArgs& a) {
   const TileCoord tc = stencil_tile(a);
   const int r0 = 2 * (tc.rhs * blockDim.x + threadIdx.x);
-  const int s = tc.site * blockDim.y + threadIdx.y;
-  const bool site_ok = s < a.g.Vh;
+  const int s = stencil_site0(a, tc) + threadIdx.y;
+  const bool site_ok = s < stencil_slim(a);
   const bool has1 = r0 + 1 < a.nrhs;
   const bool v0 = site_ok && r0 < a.nrhs && (a.active == nullptr || a.active[r0]);
   const bool v1 = site_ok && has1 && (a.active == nullptr || a.active[r0 + 1]);

@@ -48,6 +48,11 @@ struct DslashArgs {
   // tiles of a site tile adjacent (blockIdx.x = site tile * nslab + RHS tile);
   // 0: two-dimensional grid (blockIdx.x site tile, blockIdx.y RHS tile)
   int nslab;
+  // The launch covers sites [s_off, s_lim) (s_lim 0: the lattice's Vh). When
+  // several launches over disjoint site ranges share one reduction, this
+  // launch's site tiles are tiles tile_off ... of tile_total, and block_total
+  // counts the blocks of all of them (0: this launch alone).
+  int s_off, s_lim, tile_off, tile_total, block_total;
   ReduceArgs red;
   // EPI_CGXR: solution and residual in the accumulator precision (double for
   // FP64 spinors, else single), search direction in the spinor precision
@@ -77,11 +82,22 @@ inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }
 
 // The (site tile, RHS tile) of this block of a stencil launch.
 QCU_D TileCoord stencil_tile(const DslashArgs& a) {
+  TileCoord t = TileCoord::from_grid();
   if (a.nslab > 0) {
     const int st = blockIdx.x / a.nslab;
-    return TileCoord{st, (int)(gridDim.x / a.nslab), (int)(blockIdx.x - st * a.nslab)};
+    t = TileCoord{st, (int)(gridDim.x / a.nslab), (int)(blockIdx.x - st * a.nslab), gridDim.x};
   }
-  return TileCoord::from_grid();
+  if (a.block_total > 0) {
+    t.site += a.tile_off;
+    t.nsite = a.tile_total;
+    t.nblocks = (unsigned)a.block_total;
+  }
+  return t;
 }
+// first site of this block's tile and one past the launch's last site
+QCU_D int stencil_site0(const DslashArgs& a, const TileCoord& t) {
+  return a.s_off + (t.site - (a.block_total > 0 ? a.tile_off : 0)) * (int)blockDim.y;
+}
+QCU_D int stencil_slim(const DslashArgs& a) { return a.s_lim > 0 ? a.s_lim : a.g.Vh; }
 
 }  // namespace qcu

@@ -32,9 +32,15 @@ constexpr int kMaxWarps = 8;
 
 // The block's place in a (site tile, RHS tile) launch grid: by default
 // blockIdx.x / gridDim.x over site tiles and blockIdx.y over RHS tiles.
+// nblocks: the blocks that take part in the reduction (the last of them to
+// finish sums the partials); more than the launch's own when several launches
+// over disjoint sites share one reduction.
 struct TileCoord {
   int site, nsite, rhs;
-  static QCU_D TileCoord from_grid() { return TileCoord{(int)blockIdx.x, (int)gridDim.x, (int)blockIdx.y}; }
+  unsigned nblocks;
+  static QCU_D TileCoord from_grid() {
+    return TileCoord{(int)blockIdx.x, (int)gridDim.x, (int)blockIdx.y, gridDim.x * gridDim.y};
+  }
 };
 
 // vals: NR values for each of the RL right-hand sides of this thread (RHS
@@ -72,7 +78,7 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   __threadfence();
   __syncthreads();
   if (tid == 0) {
-    unsigned total = gridDim.x * gridDim.y;
+    const unsigned total = t.nblocks;
     unsigned t = atomicAdd(red.ticket, 1u);
     am_last = (t == total - 1);
   }

@@ -198,9 +198,10 @@ int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& 
   // a t-slab: the input's ghost slices from the neighbouring ranks first; the
   // per-RHS sums of the launch are this slab's part, summed over the ranks
   // before the finishing functor runs
-  QCU_CHECK(dd_exchange(o.ctx, a.in, op_spinor_prec(prec), o.st));
-  QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, FIN_NONE, a, o.w->shape, o.st));
-  o.ctx->launches++;
+  QCU_CHECK(dd_stencil(o.ctx, a, op_spinor_prec(prec), o.w->shape, o.st, [&](const DslashArgs& piece) {
+    o.ctx->launches++;
+    return launch_dslash(prec, dag, epi, FIN_NONE, piece, o.w->shape, o.st);
+  }));
   if (epi & (EPI_NORM | EPI_CGXR)) {
     QCU_CHECK(dd_sum(o.ctx, a.red.result, a.nrhs, o.st));
     if (fin != FIN_NONE) {

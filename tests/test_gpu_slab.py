@@ -27,6 +27,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 L = (8, 8, 8, 16)
 GSEED, EPS, PSEED = 11, 0.4, 5
 KAPPA, CSW, BC = 0.13, 1.0, -1.0
+KAPPAS2 = (0.125, 0.1375)
 
 
 def whole_lattice(q, torch):
@@ -53,6 +54,14 @@ def whole_lattice(q, torch):
             rep = c.invert(x, psi, kappa=KAPPA, csw=CSW, bc_t=BC, tol=1e-10, precision=prec)[0]
             assert rep["converged"]
             res["x_" + prec] = x.cpu().numpy().reshape(2, V // 2, 12)
+        # a batch of two sources with two kappas (the batched kernels and their faces)
+        bb = torch.empty(2 * V * 12, dtype=torch.complex128, device="cuda")
+        c.generate_spinor(bb, 2, PSEED + 10)
+        xb = torch.zeros_like(bb)
+        reps = c.invert(xb, bb, nrhs=2, kappas=KAPPAS2, csw=CSW, bc_t=BC, tol=1e-10, precision="half")
+        assert all(r["converged"] for r in reps)
+        res["bb"] = bb.cpu().numpy().reshape(2, 2, V // 2, 12)
+        res["xb"] = xb.cpu().numpy().reshape(2, 2, V // 2, 12)
     return res
 
 
@@ -77,6 +86,13 @@ def slab_run(q, torch, comm):
             rep = s.invert(x, psi, kappa=KAPPA, csw=CSW, bc_t=BC, tol=1e-10, precision=prec)[0]
             out["x_" + prec] = x.cpu().numpy().reshape(2, vh, 12)
             out["conv_" + prec] = rep["converged"]
+        bb = torch.empty(2 * 2 * vh * 12, dtype=torch.complex128, device="cuda")
+        s.generate_spinor(bb, 2, PSEED + 10)
+        xb = torch.zeros_like(bb)
+        reps = s.invert(xb, bb, nrhs=2, kappas=KAPPAS2, csw=CSW, bc_t=BC, tol=1e-10, precision="half")
+        out["bb"] = bb.cpu().numpy().reshape(2, 2, vh, 12)
+        out["xb"] = xb.cpu().numpy().reshape(2, 2, vh, 12)
+        out["conv_b"] = all(r["converged"] for r in reps)
         out["t0"] = s.t0
         out["vh"] = vh
     return out
@@ -100,6 +116,18 @@ def check_against_whole(oracle, whole, parts):
         assert res < 1e-10, (prec, res)
         xw = whole["x_" + prec].reshape(b.shape)
         assert np.linalg.norm(x - xw) / np.linalg.norm(xw) < 1e-8, prec
+    # the two-source, two-kappa batch
+    assert all(p["conv_b"] for p in parts)
+    assert np.array_equal(stitch(parts, "bb"), whole["bb"])
+    xb = stitch(parts, "xb")
+    for r, k in enumerate(KAPPAS2):
+        Ck = oracle.clover_build(whole["U"], L, k * CSW)
+        br = whole["bb"][r].reshape(2, -1, 4, 3)
+        xr = xb[r].reshape(br.shape)
+        res = np.linalg.norm(br - oracle.apply_full(xr, whole["U"], Ck, L, k, BC)) / np.linalg.norm(br)
+        assert res < 1e-10, (r, res)
+        xw = whole["xb"][r].reshape(br.shape)
+        assert np.linalg.norm(xr - xw) / np.linalg.norm(xw) < 1e-8, r
 
 
 @pytest.mark.parametrize("transport", ["host", "nccl"])
