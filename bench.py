@@ -297,6 +297,18 @@ def run_large(roof, torch, device, flush, args):
                 "fp64_s": td, "fp64_iterations": rd["iterations"], "fp64_true_residual": rd["true_residual"],
                 "speedup_vs_fp64": td / tm,
                 "solution_rel_err_mixed_vs_fp64": float(torch.linalg.norm(xm - xd) / torch.linalg.norm(xd))})
+    if not args.no_cpu_baseline:  # both solutions' true residuals by the oracle's FP64 operator
+        import numpy as np
+
+        from oracle import oracle as O
+        U = np.zeros((4, 2, V // 2, 3, 3), complex)
+        roof.export_gauge(U)
+        C = O.clover_build(U, ROOF_LATTICE, LARGE_KAPPA * CSW)
+        bh = b.cpu().numpy().reshape(2, V // 2, 4, 3)
+        nb = np.linalg.norm(bh)
+        for key, xx in (("mixed", xm), ("fp64", xd)):
+            r = bh - O.apply_full(xx.cpu().numpy().reshape(bh.shape), U, C, ROOF_LATTICE, LARGE_KAPPA, BC_T)
+            out[key + "_true_residual_by_oracle"] = float(np.linalg.norm(r) / nb)
     return out
 
 
