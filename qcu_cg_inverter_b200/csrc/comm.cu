@@ -131,15 +131,17 @@ static int comm_exchange_segs(qcu_comm c, const FaceSeg* seg, int n, cudaStream_
   // the same order on every rank: with two ranks lo == hi and the pairs match
   // in issue order (my send_lo with the peer's recv_hi); one rank sends to itself
   QCU_CHECK_NCCL(g_nccl.GroupStart());
-  for (int i = 0; i < n; i++) {
+  ncclResult_t r = ncclSuccess;  // the group is closed even when an operation fails
+  for (int i = 0; i < n && r == ncclSuccess; i++) {
     if (!seg[i].bytes) continue;
-    QCU_CHECK_NCCL(g_nccl.Send(seg[i].send_lo, seg[i].bytes, ncclChar, lo, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Recv(seg[i].recv_hi, seg[i].bytes, ncclChar, hi, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Send(seg[i].send_hi, seg[i].bytes, ncclChar, hi, c->nccl, st));
-    QCU_CHECK_NCCL(g_nccl.Recv(seg[i].recv_lo, seg[i].bytes, ncclChar, lo, c->nccl, st));
+    r = g_nccl.Send(seg[i].send_lo, seg[i].bytes, ncclChar, lo, c->nccl, st);
+    if (r == ncclSuccess) r = g_nccl.Recv(seg[i].recv_hi, seg[i].bytes, ncclChar, hi, c->nccl, st);
+    if (r == ncclSuccess) r = g_nccl.Send(seg[i].send_hi, seg[i].bytes, ncclChar, hi, c->nccl, st);
+    if (r == ncclSuccess) r = g_nccl.Recv(seg[i].recv_lo, seg[i].bytes, ncclChar, lo, c->nccl, st);
   }
-  QCU_CHECK_NCCL(g_nccl.GroupEnd());
-  return QCU_SUCCESS;
+  const ncclResult_t e = g_nccl.GroupEnd();
+  if (r != ncclSuccess) return nccl_status(r, "ncclSend/ncclRecv");
+  return nccl_status(e, "ncclGroupEnd");
 }
 
 static int comm_exchange(qcu_comm c, const void* send_lo, const void* send_hi, void* recv_lo, void* recv_hi,
