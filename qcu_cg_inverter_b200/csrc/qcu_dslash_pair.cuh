@@ -189,7 +189,12 @@ struct CloverPair {
   const float4* p0;
   const float4* p1;
   bool id0, id1;  // lane without a clover term (A = 1)
-  QCU_D float4 chunk0(int q) const { return __ldg(p0 + 32 * q); }
+  // float i of chunk q of the first lane's field. Each block loads only its
+  // own two floats of a chunk: one float4 load shared by both blocks would keep
+  // the other block's halves of all 18 chunks live (measured on B200, 24^3x48,
+  // 48 RHS: the hop + A^-1 stencil 1.200 -> 1.159 ms, spills of the fused K2
+  // 80 -> 40 bytes)
+  QCU_D float one(int q, int i) const { return __ldg(reinterpret_cast<const float*>(p0 + 32 * q) + i); }
   // float i of chunk q for each lane (scalar loads straight into the pair),
   // `id` for a lane without clover
   QCU_D float2 lanes(int q, int i, float id) const {
@@ -198,8 +203,6 @@ struct CloverPair {
     return make_float2(id0 ? id : a, id1 ? id : b);
   }
 };
-
-QCU_D float pick4(const float4& w, int i) { return i == 0 ? w.x : (i == 1 ? w.y : (i == 2 ? w.z : w.w)); }
 
 // v <- blockdiag(B0, B1) v for both lanes, block by block; per lane the order
 // of herm_apply
@@ -212,9 +215,8 @@ QCU_D void clover_apply_rp(PairSpinor& v, const CloverPair<UNI>& C) {
     for (int q = 0; q < 3; q++) {
       float2 d[2];
       if constexpr (UNI) {
-        const float4 w0 = C.chunk0(q);
-        d[0] = splat2(pick4(w0, b));
-        d[1] = splat2(pick4(w0, b + 2));
+        d[0] = splat2(C.one(q, b));
+        d[1] = splat2(C.one(q, b + 2));
       } else {
         d[0] = C.lanes(q, b, 1.f);
         d[1] = C.lanes(q, b + 2, 1.f);
@@ -233,9 +235,8 @@ QCU_D void clover_apply_rp(PairSpinor& v, const CloverPair<UNI>& C) {
         const int k = tri_index(i, j);
         float2 mre, mim;
         if constexpr (UNI) {
-          const float4 w0 = C.chunk0(3 + k);
-          mre = splat2(pick4(w0, b));
-          mim = splat2(pick4(w0, b + 2));
+          mre = splat2(C.one(3 + k, b));
+          mim = splat2(C.one(3 + k, b + 2));
         } else {
           mre = C.lanes(3 + k, b, 0.f);
           mim = C.lanes(3 + k, b + 2, 0.f);
