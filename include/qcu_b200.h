@@ -325,6 +325,12 @@ int qcuSlabGeometry(const int lattice[4], int nranks, int rank, int out[6]);
  * allocations the next one fails as out-of-memory (n < 0 disables). */
 void qcuDebugFailAllocAfter(long long n);
 
+/* Test hook: batched launches of the fast 16-bit operator on the RHS-paired
+ * kernels stage no neighbour words in shared memory (0), the t neighbours'
+ * (1), the z and t neighbours' (2), or as built (-1), from the next launch on,
+ * for the whole process. */
+void qcuDebugSetPairStage(int stage);
+
 /* Test hook: one launch of the batched stencil with epilogue flags `epi`
  * (1 A^-1 after the hop, 2 xpay, 4 A^-1 on x, 8 A^-1 after the xpay, 16 second
  * output A^-1 y, 32 per-RHS norm, 64 CG x/r update) on fields converted from

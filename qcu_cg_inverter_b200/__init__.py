@@ -135,6 +135,7 @@ def lib():
                               ctypes.POINTER(SolveReport)]),
             "qcuBenchStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d)]),
             "qcuDebugFailAllocAfter": (None, [ll]),
+            "qcuDebugSetPairStage": (None, [ctypes.c_int]),
             "qcuShiftVectorStorage": (i, [P, P, i, i, i, i, i]),
             "qcuShiftGaugeStorage": (i, [P, P, i, i, i, i, i]),
             "qcuDebugStencil": (i, [P, i, i, i, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d),

@@ -514,6 +514,11 @@ int qcuContextCreate(qcu_context* out, const int lattice[4], int device) {
     delete ctx;
     return st;
   }
+  e = prepare_staged_kernels();
+  if (e != cudaSuccess) {
+    qcuContextDestroy(ctx);
+    return cuda_status(e, "staged stencil set-up");
+  }
   // qcuDslashNoAlloc's device set-up happens here, so that its calls take no
   // device memory; a failure is reported by that entry point, not here
   if (noalloc_prepare(device) != QCU_SUCCESS) clear_error();
@@ -600,6 +605,7 @@ long long qcuContextDeviceBytes(qcu_context ctx) {
 long long qcuContextLaunchCount(qcu_context ctx) { return ctx ? ctx->launches : 0; }
 
 void qcuDebugFailAllocAfter(long long n) { set_alloc_fail_after(n); }
+void qcuDebugSetPairStage(int stage) { set_pair_stage_override(stage); }
 
 int qcuLoadGauge(qcu_context ctx, const void* gauge) {
   clear_error();

@@ -1,5 +1,7 @@
 // Launcher of the fused stencil kernels (instantiated per precision in
 // dslash_f64.cu, dslash_f32.cu and dslash_f16.cu).
+#include <stdlib.h>
+
 #include "qcu_kernels.cuh"
 
 namespace qcu {
@@ -11,6 +13,8 @@ DslashKernelFn pick_f16(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x(bool dag, int epi, int fin);
 DslashKernelFn pick_f16x1(bool dag, int epi, int fin);
 DslashKernelFn pick_f16p(bool dag, int epi, int fin);
+DslashKernelFn pick_f16pt(bool dag, int epi, int fin);
+DslashKernelFn pick_f16pz(bool dag, int epi, int fin);
 DslashKernelFn pick_f64b(bool dag, int epi, int fin);
 DslashKernelFn pick_f16c1(bool dag, int epi, int fin);
 
@@ -53,6 +57,42 @@ DslashKernelFn pick_f16c1(bool dag, int epi, int fin);
 static int g_pairs_override = -1;
 void set_rhs_pairs_override(int v) { g_pairs_override = v; }
 
+// RHS-paired launches with no neighbour words staged in shared memory (0),
+// the t neighbours' (1) or the z and t neighbours' (2). The environment
+// variable QCU_PAIR_STAGE overrides the built-in choice.
+#ifndef QCU_PAIR_STAGE
+#define QCU_PAIR_STAGE 0
+#endif
+static int g_stage_override = -1;
+void set_pair_stage_override(int v) { g_stage_override = v; }
+static int pair_stage() {
+  static const int env = [] {
+    const char* e = getenv("QCU_PAIR_STAGE");
+    return e ? atoi(e) : -1;
+  }();
+  const int v = g_stage_override >= 0 ? g_stage_override : env >= 0 ? env : QCU_PAIR_STAGE;
+  return v < 0 ? 0 : v > 2 ? 2 : v;
+}
+// Raises the dynamic shared memory limit of every staged kernel on the
+// current device to the most any launch shape asks for (two staged
+// directions, 256 thread slots); done when a context is created, so that no
+// attribute changes while launches are captured into graphs.
+cudaError_t prepare_staged_kernels() {
+  const int bytes = staged_bytes(4, 8, 32);
+  const int epis[] = {0, EPI_CPRE, EPI_XPAY, EPI_XPAY | EPI_CX, EPI_XPAY | EPI_CPOST, EPI_CPRE | EPI_XPAY,
+                      EPI_CPRE | EPI_XPAY | EPI_NORM, EPI_CPRE | EPI_XPAY | EPI_OUT2,
+                      EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM, EPI_XPAY | EPI_NORM, EPI_XPAY | EPI_CGXR};
+  for (int dag = 0; dag < 2; dag++)
+    for (int epi : epis)
+      for (int fin : {(int)FIN_NONE, (int)FIN_CG_ALPHA, (int)FIN_CG_BETA}) {
+        DslashKernelFn fn = pick_f16pz(dag != 0, epi, fin);
+        if (!fn) continue;
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+      }
+  return cudaSuccess;
+}
+
 cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape sh,
                           cudaStream_t stream) {
   const bool pairs = g_pairs_override < 0 ? QCU_RHS_PAIRS != 0 : g_pairs_override != 0;
@@ -61,6 +101,7 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
   // RHS lanes per thread: the RHS-paired kernels take a block of Rb/2 x Sb
   // threads for the same Rb x Sb tile of (RHS, site)
   int per_thread = 1;
+  int smem = 0;  // dynamic shared memory of the launch
   switch (prec) {
     case PREC_DOUBLE: fn = (QCU_F64_BATCH && a.nrhs > 1) ? pick_f64b(dagger, epi, fin) : pick_f64(dagger, epi, fin); break;
     case PREC_SINGLE: fn = pick_f32(dagger, epi, fin); break;
@@ -69,7 +110,9 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
       if (a.nrhs == 1) {
         fn = pick_f16x1(dagger, epi, fin);
       } else if (pairs && sh.Rb >= 2 && (pair_cgxr || !(epi & EPI_CGXR))) {
-        fn = pick_f16p(dagger, epi, fin);
+        const int ns = pair_stage();
+        fn = ns == 2 ? pick_f16pz(dagger, epi, fin) : ns == 1 ? pick_f16pt(dagger, epi, fin) : pick_f16p(dagger, epi, fin);
+        smem = ns ? staged_bytes(2 * ns, sh.Rb, sh.Sb) : 0;
         per_thread = 2;
       } else {
         fn = pick_f16x(dagger, epi, fin);
@@ -91,11 +134,11 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
     // clover are read from DRAM once and served from L2 to the others
     DslashArgs b = a;
     b.nslab = nslab;
-    fn<<<dim3(grid_x(nsites, sh.Sb) * nslab, 1), block, 0, stream>>>(b);
+    fn<<<dim3(grid_x(nsites, sh.Sb) * nslab, 1), block, smem, stream>>>(b);
   } else {
     DslashArgs b = a;
     b.nslab = 0;
-    fn<<<dim3(grid_x(nsites, sh.Sb), nslab), block, 0, stream>>>(b);
+    fn<<<dim3(grid_x(nsites, sh.Sb), nslab), block, smem, stream>>>(b);
   }
   return cudaGetLastError();
 }

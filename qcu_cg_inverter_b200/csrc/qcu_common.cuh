@@ -263,7 +263,16 @@ enum OpVariant : int {
   // the storage of OP_HALF (everything 16-bit); the kernels its single-RHS
   // launches use (paired decode, block-paired epilogues)
   OP_HALF_1 = 7,
+  // the kernels of OP_HALF_FAST_2 with the t neighbours' words (8), or the z
+  // and t neighbours' (9), staged in shared memory
+  OP_HALF_FAST_2T = 8,
+  OP_HALF_FAST_2Z = 9,
 };
+// staged directions of an RHS-paired kernel family
+__host__ __device__ constexpr int op_staged(int op) {
+  return op == OP_HALF_FAST_2T ? 1 : op == OP_HALF_FAST_2Z ? 2 : 0;
+}
+__host__ __device__ constexpr bool op_pair(int op) { return op == OP_HALF_FAST_2 || op_staged(op) > 0; }
 // Storage of the sloppy solver's accumulators (the partial solution x_lo and
 // the iterated residual r) for a sloppy spinor precision: FP64 for FP64, FP32
 // for FP32, and for 16-bit solves 16-bit like their other spinors (QCU_ACC16
@@ -279,7 +288,7 @@ __host__ __device__ constexpr int acc_prec(int ps) {
   return ps == PREC_DOUBLE ? (int)PREC_DOUBLE : (ps == PREC_HALF && QCU_ACC16) ? (int)PREC_HALF : (int)PREC_SINGLE;
 }
 __host__ __device__ constexpr bool op_fast(int op) {
-  return op == OP_HALF_FAST || op == OP_HALF_FAST_1 || op == OP_HALF_FAST_2;
+  return op == OP_HALF_FAST || op == OP_HALF_FAST_1 || op_pair(op);
 }
 __host__ __device__ constexpr int op_base(int op) {
   return op == OP_DOUBLE_BATCH ? (int)OP_DOUBLE : op == OP_HALF_1 ? (int)OP_HALF : op;

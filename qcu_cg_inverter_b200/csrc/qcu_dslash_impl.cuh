@@ -57,7 +57,7 @@ typedef void (*DslashKernelFn)(const DslashArgs);
 #ifndef QCU_DSLASH_MINB_PAIR_OUT2
 #define QCU_DSLASH_MINB_PAIR_OUT2 QCU_DSLASH_MINB_PAIR
 #endif
-constexpr int dslash_maxt(int op) { return op == OP_HALF_FAST_2 ? 128 : 256; }
+constexpr int dslash_maxt(int op) { return op_pair(op) ? 128 : 256; }
 // the compact single-RHS family (OP_HALF_1): 128 registers. Measured at
 // 32^3x64 against the 85-register cap (80 used, 28 B spilled): K2 170 vs 164
 // us, K4 134 vs 136 us, the solve 29.1 vs 29.2 ms - even, so no cap
@@ -74,7 +74,7 @@ constexpr int dslash_minb(int op, int epi) {
   return op == OP_HALF_1 ? QCU_DSLASH_MINB_C1
          : op == OP_DOUBLE ? QCU_DSLASH_MINB64
          : op == OP_DOUBLE_BATCH ? QCU_DSLASH_MINB64_BATCH
-         : op == OP_HALF_FAST_2 ? ((epi & EPI_OUT2) ? QCU_DSLASH_MINB_PAIR_OUT2 : QCU_DSLASH_MINB_PAIR)
+         : op_pair(op) ? ((epi & EPI_OUT2) ? QCU_DSLASH_MINB_PAIR_OUT2 : QCU_DSLASH_MINB_PAIR)
          : (op_spinor_prec(op) != PREC_HALF || ((op == OP_HALF_FAST_1 || op == OP_HALF_1) && !QCU_DSLASH_CAP_1RHS))
              ? QCU_DSLASH_MINB
          : (epi & EPI_OUT2)              ? QCU_DSLASH_MINB16_OUT2
@@ -247,12 +247,12 @@ QCU_D void dslash_site_body(const DslashArgs& a) {
 }
 
 // OP selects the storage of spinors, links and clover (OpVariant), and for the
-// fast 16-bit storage the kernel family: OP_HALF_FAST_2 serves two RHS per
+// fast 16-bit storage the kernel family: OP_HALF_FAST_2(T, Z) serve two RHS per
 // thread (qcu_dslash_pair.cuh), the others one.
 template <int OP, bool DAG, int EPI, class Fin>
 __global__ void __launch_bounds__(dslash_maxt(OP), dslash_minb(OP, EPI)) dslash_kernel(const DslashArgs a) {
-  if constexpr (OP == OP_HALF_FAST_2)
-    dslash_pair_body<DAG, EPI, Fin>(a);
+  if constexpr (op_pair(OP))
+    dslash_pair_body<op_staged(OP), DAG, EPI, Fin>(a);
   else
     dslash_site_body<OP, DAG, EPI, Fin>(a);
 }

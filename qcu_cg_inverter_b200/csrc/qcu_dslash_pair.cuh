@@ -47,12 +47,10 @@ QCU_D float2 load_words_pair(int4 w0[3], int4 w1[3], const CSpinorView& f, int s
 // the scale (norm x phase) the reconstruction applies. Same projector rows as
 // load_project_pair.
 template <int MU, bool FWD, int F>
-QCU_D float2 load_project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], float2 h1im[3], const CSpinorView& in,
-                             int sn, RhsPair rp, float phase) {
+QCU_D float2 project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], float2 h1im[3], const int4 w0[3],
+                        const int4 w1[3], float2 nm, float phase) {
   constexpr int S = FWD ? -F : F;
   constexpr float fS = (float)S;
-  int4 w0[3], w1[3];
-  const float2 nm = load_words_pair(w0, w1, in, sn, rp);
   const float2 sc = fmul2(nm, splat2(kInvFix * phase));
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -86,6 +84,65 @@ QCU_D float2 load_project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], flo
     }
   }
   return sc;
+}
+
+// ---------------------------------------------------------------------------
+// Staged neighbour words. At its start each thread copies the words and norms
+// of its far neighbours (t; or z and t) for both lanes into its own slots of
+// shared memory with cp.async, computes the other hops from global memory
+// meanwhile, waits for its own copies and reads those hops from its slots:
+// the far neighbours' loads are in flight from the start without holding
+// registers. Slot set k (fwd, bwd of each staged direction): words
+// [k][chunk][lane][thread], norms [k][lane][thread], so a warp's accesses are
+// consecutive 16- or 4-byte words.
+// ---------------------------------------------------------------------------
+extern __shared__ int4 qcu_staged[];  // dynamic shared memory of the staged kernels
+
+// NT slot sets of the block's threads
+template <int NT>
+struct StagedTiles {
+  int tid, nth;  // thread of the block, threads of the block
+  QCU_D int4* w(int k, int j) const { return qcu_staged + (k * 6 + j) * nth + tid; }
+  QCU_D float* n(int k, int lane) const {
+    return reinterpret_cast<float*>(qcu_staged + NT * 6 * nth) + (k * 2 + lane) * nth + tid;
+  }
+};
+
+QCU_D void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+QCU_D void cp_async4(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+QCU_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// both lanes' words and norms of site sn into the thread's slot set k
+template <int NT>
+QCU_D void stage_site(const StagedTiles<NT>& T, int k, const CSpinorView& f, int sn, RhsPair rp) {
+  const int4* p = static_cast<const int4*>(f.data);
+  const unsigned i0 = (unsigned)chunk_index(0, sn, rp.r0, 3, f.nrhs);
+  const unsigned cs = 32u * (unsigned)f.nrhs;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    cp_async16(T.w(k, 2 * c), p + i0 + c * cs);
+    cp_async16(T.w(k, 2 * c + 1), p + i0 + c * cs + rp.d);
+  }
+  const unsigned n0 = (unsigned)site_rhs_index(sn, rp.r0, f.nrhs);
+  cp_async4(T.n(k, 0), f.norm + n0);
+  cp_async4(T.n(k, 1), f.norm + n0 + rp.d);
+}
+
+// both lanes' words of the thread's slot set k; returns the norms
+template <int NT>
+QCU_D float2 load_words_staged(int4 w0[3], int4 w1[3], const StagedTiles<NT>& T, int k) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w0[c] = *T.w(k, 2 * c);
+    w1[c] = *T.w(k, 2 * c + 1);
+  }
+  return make_float2(*T.n(k, 0), *T.n(k, 1));
 }
 
 // row i of U h (FWD) or U^dag h for one half-spinor component, both lanes;
@@ -153,31 +210,49 @@ QCU_D void mul_reconstruct_rp(PairSpinor& o, const Link<float>& U, const float2 
   }
 }
 
-template <int MU, int F>
+// Both hops of direction MU. kst >= 0: the neighbours' words come from the
+// thread's staged slots kst (forward) and kst + 1 (backward)
+template <int MU, int F, int NT = 2>
 QCU_D void hop_dir_rp(PairSpinor& o, const Geom& g, const Nbrs& nb, int parity, int s, RhsPair rp,
-                      const CSpinorView& in, const void* gauge, float bc_t) {
+                      const CSpinorView& in, const void* gauge, float bc_t, const StagedTiles<NT>* T = nullptr,
+                      int kst = -1) {
   Link<float> U;
+  int4 w0[3], w1[3];
   float2 h0re[3], h0im[3], h1re[3], h1im[3];
   LinkIO<LINK_SINGLE18>::load(U, gauge, g.Vh_pad, MU, parity, s);
-  float2 sc = load_project_rp<MU, true, F>(h0re, h0im, h1re, h1im, in, nb.fwd[MU], rp,
-                                           (MU == 3 && nb.tf) ? bc_t : 1.f);
+  float2 nm = kst >= 0 ? load_words_staged(w0, w1, *T, kst) : load_words_pair(w0, w1, in, nb.fwd[MU], rp);
+  float2 sc = project_rp<MU, true, F>(h0re, h0im, h1re, h1im, w0, w1, nm, (MU == 3 && nb.tf) ? bc_t : 1.f);
   mul_reconstruct_rp<MU, true, F>(o, U, h0re, h0im, h1re, h1im, sc);
   LinkIO<LINK_SINGLE18>::load(U, gauge, g.Vh_pad, MU, 1 - parity, nb.bwd[MU]);
-  sc = load_project_rp<MU, false, F>(h0re, h0im, h1re, h1im, in, nb.bwd[MU], rp, (MU == 3 && nb.tb) ? bc_t : 1.f);
+  nm = kst >= 0 ? load_words_staged(w0, w1, *T, kst + 1) : load_words_pair(w0, w1, in, nb.bwd[MU], rp);
+  sc = project_rp<MU, false, F>(h0re, h0im, h1re, h1im, w0, w1, nm, (MU == 3 && nb.tb) ? bc_t : 1.f);
   mul_reconstruct_rp<MU, false, F>(o, U, h0re, h0im, h1re, h1im, sc);
 }
 
-template <bool DAG>
-QCU_D void hop_rp(PairSpinor& o, const Geom& g, int parity, int s, RhsPair rp, const CSpinorView& in,
-                  const void* gauge, float bc_t) {
+// The hop D (or D^dag) of both lanes, in the order x, y, z, t. NS > 0: the
+// last NS directions read staged slots, after the thread has waited for them
+// (HALF = 1: directions up to 3 - NS; HALF = 2: the rest; HALF = 0: all four
+// from global memory).
+template <bool DAG, int NS, int HALF>
+QCU_D void hop_rp(PairSpinor& o, const Geom& g, const Nbrs& nb, int parity, int s, RhsPair rp,
+                  const CSpinorView& in, const void* gauge, float bc_t,
+                  const StagedTiles<2 * (NS > 0 ? NS : 1)>* T = nullptr) {
   constexpr int F = DAG ? -1 : 1;
+  if constexpr (HALF != 2) {
 #pragma unroll
-  for (int k = 0; k < 12; k++) o.re[k] = o.im[k] = make_float2(0.f, 0.f);
-  const Nbrs nb = neighbours(g, s, parity);
-  hop_dir_rp<0, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
-  hop_dir_rp<1, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
-  hop_dir_rp<2, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
-  hop_dir_rp<3, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+    for (int k = 0; k < 12; k++) o.re[k] = o.im[k] = make_float2(0.f, 0.f);
+  }
+  constexpr int first_staged = HALF == 0 ? 4 : 4 - NS;
+  if constexpr (HALF != 2) {
+    hop_dir_rp<0, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+    hop_dir_rp<1, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+    if constexpr (first_staged > 2) hop_dir_rp<2, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+    if constexpr (first_staged > 3) hop_dir_rp<3, F>(o, g, nb, parity, s, rp, in, gauge, bc_t);
+  }
+  if constexpr (HALF == 2) {
+    if constexpr (first_staged <= 2) hop_dir_rp<2, F, 2 * NS>(o, g, nb, parity, s, rp, in, gauge, bc_t, T, 0);
+    hop_dir_rp<3, F, 2 * NS>(o, g, nb, parity, s, rp, in, gauge, bc_t, T, 2 * (NS - 1));
+  }
 }
 
 // Element pair of the block-interleaved FP32 clover: chunk q of the lanes'
@@ -372,8 +447,11 @@ QCU_D void xpay16_rp(PairSpinor& o, const CSpinorView& f, int s, RhsPair rp, flo
 
 // The kernel body: thread (threadIdx.x, threadIdx.y) of the block at tile
 // (site tile, RHS tile) serves RHS pair 2*(RHS tile*blockDim.x + threadIdx.x)
-// + {0, 1} of site (site tile)*blockDim.y + threadIdx.y.
-template <bool DAG, int EPI, class Fin>
+// + {0, 1} of site (site tile)*blockDim.y + threadIdx.y. NS > 0: the hops of
+// the last NS directions (t; or z and t) read neighbour words staged in the
+// thread's slots of dynamic shared memory (staged_bytes(2 NS, 2 blockDim.x,
+// blockDim.y) bytes).
+template <int NS, bool DAG, int EPI, class Fin>
 QCU_D void dslash_pair_body(const DslashArgs& a) {
   const TileCoord tc = stencil_tile(a);
   const int r0 = 2 * (tc.rhs * blockDim.x + threadIdx.x);
@@ -385,9 +463,25 @@ QCU_D void dslash_pair_body(const DslashArgs& a) {
   const RhsPair rp{r0, has1 ? 1 : 0};
   double n0 = 0.0, n1 = 0.0;
   if (v0 || v1) {
-    const int r1 = r0 + rp.d;
     PairSpinor o;
-    hop_rp<DAG>(o, a.g, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
+    const Nbrs nb = neighbours(a.g, s, a.parity);
+    StagedTiles<2 * (NS > 0 ? NS : 1)> T;
+    if constexpr (NS > 0) {
+      T.tid = threadIdx.y * blockDim.x + threadIdx.x;
+      T.nth = blockDim.x * blockDim.y;
+#pragma unroll
+      for (int j = 0; j < NS; j++) {
+        stage_site(T, 2 * j, a.in, nb.fwd[4 - NS + j], rp);
+        stage_site(T, 2 * j + 1, a.in, nb.bwd[4 - NS + j], rp);
+      }
+      hop_rp<DAG, NS, 1>(o, a.g, nb, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
+      cp_async_wait_all();
+    }
+    const int r1 = r0 + rp.d;
+    if constexpr (NS > 0)
+      hop_rp<DAG, NS, 2>(o, a.g, nb, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t, &T);
+    else
+      hop_rp<DAG, 0, 0>(o, a.g, nb, a.parity, s, rp, a.in, a.gauge, (float)a.bc_t);
     const bool need_clov = (EPI & (EPI_CPRE | EPI_CX | EPI_CPOST | EPI_OUT2)) != 0;
     const void* c0 = need_clov ? clover_of(a, r0) : nullptr;
     const void* c1 = need_clov ? clover_of(a, r1) : nullptr;

@@ -64,6 +64,11 @@ struct DslashArgs {
 // Finishing functors available to fused reductions (see solver kernels).
 enum FinId : int { FIN_NONE = 0, FIN_CG_ALPHA = 1, FIN_CG_BETA = 2 };
 
+// shared-memory bytes of NT staged neighbours (16-bit words and norms of both
+// lanes of every thread) of a block of RB/2 x SB threads (the RHS-paired
+// kernels of qcu_dslash_pair.cuh)
+QCU_HD constexpr int staged_bytes(int NT, int RB, int SB) { return NT * SB * RB * (3 * 16 + 4); }
+
 // Launch configuration: block = (Rb rhs lanes, Sb site lanes).
 struct LaunchShape {
   int Rb, Sb;
@@ -76,6 +81,12 @@ cudaError_t launch_dslash(int op, bool dagger, int epi, int fin, const DslashArg
 // Test hook: batched launches of the fast 16-bit operator on the RHS-paired
 // kernels for every epilogue (1), on one RHS per thread (0), or as built (-1).
 void set_rhs_pairs_override(int v);
+// Test hook: staged neighbours of the RHS-paired kernels (0 none, 1 t, 2 z
+// and t, -1 as built)
+void set_pair_stage_override(int v);
+// the dynamic shared memory limit of the staged RHS-paired kernels, on the
+// current device
+cudaError_t prepare_staged_kernels();
 
 // Number of blocks along x for a field of Vh sites.
 inline int grid_x(int Vh, int Sb) { return (Vh + Sb - 1) / Sb; }

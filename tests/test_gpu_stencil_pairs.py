@@ -9,7 +9,10 @@ column, a column without clover and two clover fields, so that pairs are
 uniform, mixed (clover next to Wilson) and half-empty. Only the per-RHS norms
 may differ, in the last bits (their block sums group sites differently).
 Against the FP64 oracle the tolerance is that of 16-bit storage: 2e-4 of the
-largest component, on inputs quantised the same way."""
+largest component, on inputs quantised the same way.
+
+The paired kernels that stage the t neighbours' words (stage 1), or the z and
+t neighbours' (stage 2), in shared memory store the same bits as well."""
 import numpy as np
 import pytest
 
@@ -48,12 +51,17 @@ def run(c, epi, dag, pairs, fields, **kw):
                            out2=fields["out2"].copy() if epi & OUT2 else None, rhs_pairs=pairs, **kw)
 
 
+@pytest.mark.parametrize("stage", [0, 1, 2])
 @pytest.mark.parametrize("dag", [0, 1])
 @pytest.mark.parametrize("epi", EPILOGUES)
-def test_paired_kernels_store_the_same_bits(ctx, oracle, epi, dag):
+def test_paired_kernels_store_the_same_bits(ctx, oracle, qcu_lib, epi, dag, stage):
     c, U, L = ctx
     f = dict(zip(("in", "x", "out", "out2"), (spinors(oracle, L, 100 * k) for k in range(1, 5))))
-    a = run(c, epi, dag, 1, f)
+    qcu_lib.lib().qcuDebugSetPairStage(stage)
+    try:
+        a = run(c, epi, dag, 1, f)
+    finally:
+        qcu_lib.lib().qcuDebugSetPairStage(-1)
     b = run(c, epi, dag, 0, f)
     assert np.array_equal(a["out"], b["out"])
     if epi & OUT2:
