@@ -85,6 +85,35 @@ def test_multi_rhs_multi_kappa_equals_single(cuda, qcu_lib, oracle):
             assert np.linalg.norm(xs[r] - x1) / np.linalg.norm(x1) < 1e-8
 
 
+@pytest.mark.parametrize("stage", [1, 2])
+def test_batched_solve_with_staged_neighbours_is_bit_identical(cuda, qcu_lib, oracle, stage):
+    """The RHS-paired stencils that stage far neighbours in shared memory
+    store the same bits, so a whole batched solve (fresh context: its graphs
+    are captured with the staged kernels) gives the same solution bits and
+    iteration counts as with the unstaged kernels (both on the default launch
+    shape: the sums of the solver's reductions depend on the shape)."""
+    L = (8, 8, 8, 16)
+    U = oracle.gauge_random(L, 6, 0.4)
+    kappas = [0.1360, 0.1360, 0.1375, 0.1375, 0.1375]
+    bs = np.stack([oracle.full_spinor_random(L, 40 + r) for r in range(len(kappas))])
+    out = {}
+    for st in (0, stage):
+        qcu_lib.lib().qcuDebugSetPairStage(st)
+        try:
+            with qcu_lib.Context(L) as c:
+                c.load_gauge(dev(U))
+                xb = dev(np.zeros_like(bs))
+                reps = c.invert(xb, dev(bs), nrhs=len(kappas), kappas=kappas, csw=1.0, tol=1e-10, precision="half",
+                                autotune=0)
+                out[st] = (host(xb, bs.shape), [r["iterations"] for r in reps])
+        finally:
+            qcu_lib.lib().qcuDebugSetPairStage(-1)
+    assert np.array_equal(out[0][0], out[stage][0])
+    assert out[0][1] == out[stage][1]
+    for r, k in enumerate(kappas):
+        assert true_residual(oracle, out[stage][0][r], bs[r], U, L, k, 1.0) < 1e-10
+
+
 def test_successive_solves_with_different_parameters(cuda, qcu_lib, oracle):
     """One context, one batch size, solves that differ only in parameters the
     captured CUDA graphs would bake in (boundary, clover on/off, tolerance):
