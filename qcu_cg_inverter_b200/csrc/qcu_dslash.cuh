@@ -197,6 +197,25 @@ QCU_D float2 dec_lo2(int a, int b) {
 QCU_D float2 dec_hi2(int a, int b) {
   return fadd2(make_float2(u16f(a, 0x7432), u16f(b, 0x7432)), splat2(-8421376.0f));
 }
+// The raw 16-bit values of words a (lane 0) and b (lane 1), low or high
+// halves: 8421376 + v, integers in [2^23, 2^24).
+QCU_D float2 raw_lo2(int a, int b) { return make_float2(u16f(a, 0x7410), u16f(b, 0x7410)); }
+QCU_D float2 raw_hi2(int a, int b) { return make_float2(u16f(a, 0x7432), u16f(b, 0x7432)); }
+// p + s q per lane (s = S0, S1 = +-1) of raw values p and q, exactly, which
+// equals dec(p) + s dec(q): where s = -1 the offsets cancel in the difference
+// of two integers in [2^23, 2^24); where s = +1 twice the offset comes off p
+// first (an integer below 2^24 in magnitude) and q's offset restores one.
+// One or two paired instructions instead of the decode's two and the
+// combination's one.
+template <int S0, int S1>
+QCU_D float2 raw_comb2(float2 p, float2 q) {
+  if constexpr (S0 < 0 && S1 < 0) {
+    return ffma2(q, splat2(-1.f), p);
+  } else {
+    constexpr float c0 = S0 > 0 ? -16842752.0f : 0.f, c1 = S1 > 0 ? -16842752.0f : 0.f;
+    return ffma2(q, make_float2((float)S0, (float)S1), fadd2(p, make_float2(c0, c1)));
+  }
+}
 QCU_D int word_of(const int4 w[3], int k) {
   const int4 c = w[k >> 2];
   const int l = k & 3;
@@ -234,7 +253,6 @@ template <int PL> QCU_HD constexpr float link_unit() { return PL == LINK_HALF_RA
 template <int MU, bool FWD, int F>
 QCU_D float load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, float phase) {
   constexpr int S = FWD ? -F : F;
-  constexpr float fS = (float)S;
   constexpr bool SWAP = (MU == 0 || MU == 1);  // lower pair as (p3, p2)
   const int4* p = static_cast<const int4*>(in.data);
   int4 w[3];
@@ -246,21 +264,22 @@ QCU_D float load_project_pair(HalfPair& h, const CSpinorView& in, int s, int r, 
     // component k = 3*spin + colour; word k holds (re, im) as (lo, hi)
     const int w0 = word_of(w, c), w1 = word_of(w, 3 + c);
     const int w2 = word_of(w, SWAP ? 9 + c : 6 + c), w3 = word_of(w, SWAP ? 6 + c : 9 + c);
-    const float2 Pre = dec_lo2(w0, w1), Pim = dec_hi2(w0, w1);
-    const float2 Qre = dec_lo2(w2, w3), Qim = dec_hi2(w2, w3);
+    // raw values; the combinations below are exact, as with decoded values
+    const float2 Pre = raw_lo2(w0, w1), Pim = raw_hi2(w0, w1);
+    const float2 Qre = raw_lo2(w2, w3), Qim = raw_hi2(w2, w3);
     float2 hre, him;
     if constexpr (MU == 0) {  // h0 = p0 + S i p3, h1 = p1 + S i p2; Q = (p3, p2)
-      hre = ffma2(Qim, splat2(-fS), Pre);
-      him = ffma2(Qre, splat2(fS), Pim);
+      hre = raw_comb2<-S, -S>(Pre, Qim);
+      him = raw_comb2<S, S>(Pim, Qre);
     } else if constexpr (MU == 1) {  // h0 = p0 - S p3, h1 = p1 + S p2; Q = (p3, p2)
-      hre = ffma2(Qre, make_float2(-fS, fS), Pre);
-      him = ffma2(Qim, make_float2(-fS, fS), Pim);
+      hre = raw_comb2<-S, S>(Pre, Qre);
+      him = raw_comb2<-S, S>(Pim, Qim);
     } else if constexpr (MU == 2) {  // h0 = p0 + S i p2, h1 = p1 - S i p3; Q = (p2, p3)
-      hre = ffma2(Qim, make_float2(-fS, fS), Pre);
-      him = ffma2(Qre, make_float2(fS, -fS), Pim);
+      hre = raw_comb2<-S, S>(Pre, Qim);
+      him = raw_comb2<S, -S>(Pim, Qre);
     } else {  // h0 = p0 + S p2, h1 = p1 + S p3; Q = (p2, p3)
-      hre = ffma2(Qre, splat2(fS), Pre);
-      him = ffma2(Qim, splat2(fS), Pim);
+      hre = raw_comb2<S, S>(Pre, Qre);
+      him = raw_comb2<S, S>(Pim, Qim);
     }
     h.re[c] = hre;
     h.im[c] = him;

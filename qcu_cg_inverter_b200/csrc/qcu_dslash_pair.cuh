@@ -50,37 +50,36 @@ template <int MU, bool FWD, int F>
 QCU_D float2 project_rp(float2 h0re[3], float2 h0im[3], float2 h1re[3], float2 h1im[3], const int4 w0[3],
                         const int4 w1[3], float2 nm, float phase) {
   constexpr int S = FWD ? -F : F;
-  constexpr float fS = (float)S;
   const float2 sc = fmul2(nm, splat2(kInvFix * phase));
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    float2 pre[4], pim[4];
+    float2 pre[4], pim[4];  // raw values (raw_comb2 combines them exactly)
 #pragma unroll
     for (int sp = 0; sp < 4; sp++) {
       const int a = word_of(w0, 3 * sp + c), b = word_of(w1, 3 * sp + c);
-      pre[sp] = dec_lo2(a, b);
-      pim[sp] = dec_hi2(a, b);
+      pre[sp] = raw_lo2(a, b);
+      pim[sp] = raw_hi2(a, b);
     }
     if constexpr (MU == 0) {  // h0 = p0 + S i p3, h1 = p1 + S i p2
-      h0re[c] = ffma2(pim[3], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pre[3], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pim[2], splat2(-fS), pre[1]);
-      h1im[c] = ffma2(pre[2], splat2(fS), pim[1]);
+      h0re[c] = raw_comb2<-S, -S>(pre[0], pim[3]);
+      h0im[c] = raw_comb2<S, S>(pim[0], pre[3]);
+      h1re[c] = raw_comb2<-S, -S>(pre[1], pim[2]);
+      h1im[c] = raw_comb2<S, S>(pim[1], pre[2]);
     } else if constexpr (MU == 1) {  // h0 = p0 - S p3, h1 = p1 + S p2
-      h0re[c] = ffma2(pre[3], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pim[3], splat2(-fS), pim[0]);
-      h1re[c] = ffma2(pre[2], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pim[2], splat2(fS), pim[1]);
+      h0re[c] = raw_comb2<-S, -S>(pre[0], pre[3]);
+      h0im[c] = raw_comb2<-S, -S>(pim[0], pim[3]);
+      h1re[c] = raw_comb2<S, S>(pre[1], pre[2]);
+      h1im[c] = raw_comb2<S, S>(pim[1], pim[2]);
     } else if constexpr (MU == 2) {  // h0 = p0 + S i p2, h1 = p1 - S i p3
-      h0re[c] = ffma2(pim[2], splat2(-fS), pre[0]);
-      h0im[c] = ffma2(pre[2], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pim[3], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pre[3], splat2(-fS), pim[1]);
+      h0re[c] = raw_comb2<-S, -S>(pre[0], pim[2]);
+      h0im[c] = raw_comb2<S, S>(pim[0], pre[2]);
+      h1re[c] = raw_comb2<S, S>(pre[1], pim[3]);
+      h1im[c] = raw_comb2<-S, -S>(pim[1], pre[3]);
     } else {  // h0 = p0 + S p2, h1 = p1 + S p3
-      h0re[c] = ffma2(pre[2], splat2(fS), pre[0]);
-      h0im[c] = ffma2(pim[2], splat2(fS), pim[0]);
-      h1re[c] = ffma2(pre[3], splat2(fS), pre[1]);
-      h1im[c] = ffma2(pim[3], splat2(fS), pim[1]);
+      h0re[c] = raw_comb2<S, S>(pre[0], pre[2]);
+      h0im[c] = raw_comb2<S, S>(pim[0], pim[2]);
+      h1re[c] = raw_comb2<S, S>(pre[1], pre[3]);
+      h1im[c] = raw_comb2<S, S>(pim[1], pim[3]);
     }
   }
   return sc;
