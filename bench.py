@@ -275,8 +275,8 @@ def run_large(roof, torch, device, flush, args):
     stream = torch.cuda.ExternalStream(roof.stream, device=device)
     kw = dict(kappa=LARGE_KAPPA, csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta)
 
-    def solve(prec):
-        rep = roof.invert(x, b, precision=prec, **kw)[0]
+    def solve(prec):  # --delta applies to the mixed-precision solve only
+        rep = roof.invert(x, b, precision=prec, **(kw if prec != "double" else dict(kw, delta=0.0)))[0]
         assert rep["converged"], rep
         return rep
 
@@ -349,8 +349,8 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     kw = dict(kappa=KAPPA, csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta)
 
-    def solve(xx, bb, prec):
-        rep = ctx.invert(xx, bb, precision=prec, **kw)[0]
+    def solve(xx, bb, prec):  # --delta applies to the mixed-precision solve only
+        rep = ctx.invert(xx, bb, precision=prec, **(kw if prec != "double" else dict(kw, delta=0.0)))[0]
         assert rep["converged"], rep
         return rep
 
@@ -582,6 +582,7 @@ def run_multi(args, check_oracle=False):
     kap = [k for k in MULTI_KAPPAS for _ in range(12)]
     x = torch.zeros_like(b)
     kw = dict(csw=CSW, bc_t=BC_T, tol=TOL, delta=args.delta)
+    kw64 = dict(kw, delta=0.0)  # --delta applies to the mixed-precision batch only
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
 
     def timed(fn):
@@ -619,13 +620,13 @@ def run_multi(args, check_oracle=False):
                 oracle_res.append(float(np.linalg.norm(res) / np.linalg.norm(br)))
     # FP64 single-RHS sample: spin-colour 0 for each kappa
     x1 = torch.zeros_like(b[0])
-    ctx.invert(x1, b[0].contiguous(), kappa=MULTI_KAPPAS[0], precision="double", **kw)
+    ctx.invert(x1, b[0].contiguous(), kappa=MULTI_KAPPAS[0], precision="double", **kw64)
     t64, it64 = [], []
     for j, k in enumerate(MULTI_KAPPAS):
         bb = b[12 * j].contiguous()
         ts = []
         for _ in range(2):  # two timings per kappa, the faster one kept
-            t, r = timed(lambda: ctx.invert(x1, bb, kappa=k, precision="double", **kw)[0])
+            t, r = timed(lambda: ctx.invert(x1, bb, kappa=k, precision="double", **kw64)[0])
             assert r["converged"], r
             ts.append(t)
         t64.append(min(ts))
@@ -685,7 +686,7 @@ def run_serve(args):
     import qcu_cg_inverter_b200 as q
     device = torch.device("cuda", 0)
     srv = q.Server(0, columns=args.columns, clover_slots=args.clover_slots, tol=TOL, bc_t=BC_T,
-                   precision=q._PREC[args.precision], max_chunk=args.max_chunk)
+                   precision=q._PREC[args.precision], max_chunk=args.max_chunk, delta=args.delta)
     cids = {}
     for li, L in enumerate(SERVE_LATTICES):
         for c in range(3):

@@ -102,8 +102,8 @@ typedef struct {
 } qcu_solve_report;
 
 /* Fills params with the defaults: kappa 0.12, csw 0, bc_t -1, tol 1e-10,
- * maxiter 20000, precision half, delta 0 (= 1e-2 for 16-bit inner storage,
- * 1e-3 for single and double), use_graphs 1, autotune 1. */
+ * maxiter 20000, precision half, delta 0 (= 2e-3 for 16-bit inner storage,
+ * 1e-3 for single, 1e-12 for double), use_graphs 1, autotune 1. */
 void qcuSolveParamsDefault(qcu_solve_params* params);
 
 int qcuContextCreate(qcu_context* ctx, const int lattice[4], int device);
