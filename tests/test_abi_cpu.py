@@ -76,10 +76,15 @@ def test_calls_before_init_report_not_initialized(qcu_lib):
     assert qcu_lib.last_error()[0] == qcu_lib.QCU_ERR_NOT_INITIALIZED
 
 
-def test_bad_lattice_rejected(qcu_lib):
+@pytest.mark.parametrize("lattice", [(7, 8, 8, 8), (8, 0, 8, 8), (8, 8, -2, 8), (128, 128, 128, 256)],
+                         ids=["odd-Lx", "zero-extent", "negative-extent", "beyond-32-bit-fields"])
+def test_bad_lattice_rejected(qcu_lib, lattice):
+    """Rejected before any device call: odd Lx, empty or negative extents, and
+    a half volume whose 12-chunk spinor field would pass 2^30 chunks."""
     h = ctypes.c_void_p()
-    L4 = (ctypes.c_int * 4)(7, 8, 8, 8)  # odd Lx
+    L4 = (ctypes.c_int * 4)(*lattice)
     assert qcu_lib.lib().qcuContextCreate(ctypes.byref(h), L4, 0) == qcu_lib.QCU_ERR_INVALID_ARG
+    assert not h.value
 
 
 def test_server_param_defaults(qcu_lib):

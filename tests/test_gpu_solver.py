@@ -134,6 +134,36 @@ def test_successive_solves_with_different_parameters(cuda, qcu_lib, oracle):
             assert rep["converged"] and res < kw["tol"], (kw, rep, res)
 
 
+def test_bad_solve_arguments_are_rejected(cuda, qcu_lib, oracle):
+    """Empty batches, non-positive or non-finite kappa, a zero tolerance, and a
+    batch whose fields would pass 2^32 chunks: each returns INVALID_ARG and
+    leaves the context usable."""
+    import ctypes
+    q = qcu_lib
+    L = (8, 8, 8, 8)
+    b = oracle.full_spinor_random(L, 4)
+    with q.Context(L) as c:
+        c.generate_gauge(1, 0.3)
+        x, bd = dev(np.zeros_like(b)), dev(b)
+        sp = q.solve_params(kappa=0.12)
+        reps = (q.SolveReport * 1)()
+        assert q.lib().qcuInvert(c._h, q._ptr(x), q._ptr(bd), 0, None, ctypes.byref(sp), reps) == q.QCU_ERR_INVALID_ARG
+        for kw in (dict(kappa=0.0), dict(kappa=-0.1), dict(kappa=float("nan")), dict(kappa=0.12, tol=0.0)):
+            with pytest.raises(q.QcuError) as e:
+                c.invert(x, bd, **kw)
+            assert e.value.code == q.QCU_ERR_INVALID_ARG, kw
+        rep = c.invert(x, bd, kappa=0.12, csw=1.0)[0]
+        assert rep["converged"]
+    big = (32, 32, 32, 64)  # 1048576 sites per parity x 12 chunks x 400 RHS > 2^32
+    with q.Context(big) as c:
+        c.generate_gauge(1, 0.3)
+        one = dev(np.zeros(1, complex))
+        sp = q.solve_params(kappa=0.12)
+        reps = (q.SolveReport * 400)()
+        code = q.lib().qcuInvert(c._h, q._ptr(one), q._ptr(one), 400, None, ctypes.byref(sp), reps)
+        assert code == q.QCU_ERR_INVALID_ARG
+
+
 def test_nan_source_is_rejected(cuda, qcu_lib, oracle):
     L = (8, 8, 8, 8)
     b = oracle.full_spinor_random(L, 4)
