@@ -26,37 +26,6 @@ template <class R> QCU_D double norm2(const Spinor<R>& v) {
   return n;
 }
 
-// x += alpha p ; r -= alpha z ; rr = |r|^2 -> FinCgBeta
-template <int PA, int PS>
-__global__ void __launch_bounds__(256) cg_xr_kernel(int nsites, int nrhs, SpinorView x, SpinorView rv, CSpinorView p,
-                                                    CSpinorView z, const double* alpha, const int* active, ReduceArgs red) {
-  typedef typename CompReal<PA>::type RA;
-  typedef typename CompReal<PS>::type RS;
-  QCU_SITE_RHS
-  double nrm = 0.0;
-  if (valid) {
-    const RA a = (RA)alpha[r];
-    Spinor<RA> xv, rr;
-    Spinor<RS> pv, zv;
-    SpinorIO<PA>::load(xv, x, s, r);
-    SpinorIO<PA>::load(rr, rv, s, r);
-    SpinorIO<PS>::load(pv, p, s, r);
-    SpinorIO<PS>::load(zv, z, s, r);
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-      xv.c[k].re += a * (RA)pv.c[k].re;
-      xv.c[k].im += a * (RA)pv.c[k].im;
-      rr.c[k].re -= a * (RA)zv.c[k].re;
-      rr.c[k].im -= a * (RA)zv.c[k].im;
-    }
-    SpinorIO<PA>::store(x, s, r, xv);
-    SpinorIO<PA>::store(rv, s, r, rr);
-    nrm = norm2(rr);
-  }
-  double v[1] = {nrm};
-  block_reduce_finish<1, FinCgBeta>(v, nrhs, red);
-}
-
 // p = r + beta p
 template <int PA, int PS>
 __global__ void __launch_bounds__(256) cg_p_kernel(int nsites, int nrhs, SpinorView p, CSpinorView rv,
@@ -245,19 +214,6 @@ __global__ void __launch_bounds__(256) ref_p_kernel(int nsites, SpinorView p, CS
 static inline dim3 blk(LaunchShape sh) { return dim3(sh.Rb, sh.Sb); }
 static inline dim3 grd(int nsites, int nrhs, LaunchShape sh) {
   return dim3(grid_x(nsites, sh.Sb), (nrhs + sh.Rb - 1) / sh.Rb);
-}
-
-cudaError_t launch_cg_xr(int pa, int ps, int nsites, int nrhs, SpinorView x, SpinorView r, CSpinorView p, CSpinorView z,
-                         const double* alpha, const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t st) {
-  dim3 b = blk(sh), g = grd(nsites, nrhs, sh);
-#define QCU_XR(A, S) cg_xr_kernel<A, S><<<g, b, 0, st>>>(nsites, nrhs, x, r, p, z, alpha, active, red)
-  if (pa == PREC_DOUBLE && ps == PREC_DOUBLE) QCU_XR(PREC_DOUBLE, PREC_DOUBLE);
-  else if (pa == PREC_SINGLE && ps == PREC_SINGLE) QCU_XR(PREC_SINGLE, PREC_SINGLE);
-  else if (pa == PREC_SINGLE && ps == PREC_HALF) QCU_XR(PREC_SINGLE, PREC_HALF);
-  else if (pa == PREC_HALF && ps == PREC_HALF) QCU_XR(PREC_HALF, PREC_HALF);
-  else return cudaErrorInvalidValue;
-#undef QCU_XR
-  return cudaGetLastError();
 }
 
 cudaError_t launch_cg_p(int pa, int ps, int nsites, int nrhs, SpinorView p, CSpinorView r, const double* beta,

@@ -251,8 +251,6 @@ cudaError_t launch_clover_build(const Geom& g, const void* gauge64, double csw_e
 cudaError_t launch_clover_apply(int prec, const Geom& g, int parity, int nrhs, CSpinorView in, SpinorView out,
                                 const void* clov, size_t clov_stride, const int* clov_idx, const int* active,
                                 const ReduceArgs* red, LaunchShape sh, cudaStream_t stream);
-cudaError_t launch_cg_xr(int pa, int ps, int nsites, int nrhs, SpinorView x, SpinorView r, CSpinorView p, CSpinorView z,
-                         const double* alpha, const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
 cudaError_t launch_cg_p(int pa, int ps, int nsites, int nrhs, SpinorView p, CSpinorView r, const double* beta,
                         const int* active, LaunchShape sh, cudaStream_t st);
 cudaError_t launch_convert(int pd, int psrc, int nsites, int nrhs, SpinorView dst, CSpinorView src, const int* active,
