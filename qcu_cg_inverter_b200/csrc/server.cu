@@ -27,6 +27,14 @@
 
 #include "qcu_engine.h"
 
+// reliable-update pause alignment of the server's engines (EngineParams::align).
+// Measured on B200 with chunk gathering and delta 2e-3, serving stream (two
+// runs each): 1 -> 327.5, 326.9; 3 -> 327.7, 328.6; 8 -> 329.6, 329.0;
+// 24 -> 328.6, 327.1 RHS solves/s
+#ifndef QCU_SERVER_ALIGN
+#define QCU_SERVER_ALIGN 8.0
+#endif
+
 using namespace qcu;
 
 extern "C" void qcu_solver_workspace_free(qcu_context ctx);  // engine.cu
@@ -168,7 +176,7 @@ int make_resident(qcu_server_s* s, int id) {
     ep.clover = true;
     ep.graphs = true;
     ep.max_chunk = s->P.max_chunk > 0 ? s->P.max_chunk : 8;
-    ep.align = 8.0;
+    ep.align = QCU_SERVER_ALIGN;
     st = eng->configure(ctx, s->P.columns, ep);
   }
   if (st == QCU_SUCCESS) {
