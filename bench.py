@@ -425,7 +425,7 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": world * steps / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": V * 12 * 16,
                     "d2h_bytes_per_step": V * 12 * 16},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_source": src,
+                         "peak_source": src, "frac_of_nominal_8000_GBps": achieved / 8000.0,
                          "traffic": tps * (V_roof // 2) if tps else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                                            "per site, times the sites of this launch",
