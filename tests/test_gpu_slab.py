@@ -1,7 +1,7 @@
 """Domain decomposition along t on the GPU (SlabContext).
 
-One GPU serves these tests, so the multi-rank case runs two processes on it
-with the host transport (their kernels never wait on one another: the halo
+One GPU serves these tests, so the multi-rank cases run two or four
+processes on it with the host transport (their kernels never wait on one another: the halo
 exchange and the sums go through the host, over a gloo process group). The
 NCCL transport runs with one rank, which sends its faces to itself.
 
@@ -170,12 +170,16 @@ def _rank_main(rank, world, port, out_path):
     dist.destroy_process_group()
 
 
-def test_two_ranks_on_one_gpu_equal_whole_lattice(cuda, qcu_lib, oracle, tmp_path):
+@pytest.mark.parametrize("world", [2, 4])
+def test_ranks_on_one_gpu_equal_whole_lattice(cuda, qcu_lib, oracle, tmp_path, world):
+    """world processes on the one GPU over the host transport. With 2 ranks
+    each rank's two neighbours are the same rank; with 4 (slabs of 4 time
+    slices) every rank exchanges with two different ranks."""
     import torch
     import torch.multiprocessing as mp
     whole = whole_lattice(qcu_lib, torch)
     out = str(tmp_path / "slab")
-    mp.spawn(_rank_main, args=(2, _free_port(), out), nprocs=2, join=True)
-    parts = [dict(np.load(f"{out}.{r}.npz")) for r in range(2)]
-    assert [int(p["t0"]) for p in parts] == [0, 8]
+    mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
+    parts = [dict(np.load(f"{out}.{r}.npz")) for r in range(world)]
+    assert [int(p["t0"]) for p in parts] == [r * L[3] // world for r in range(world)]
     check_against_whole(oracle, whole, parts)
