@@ -846,7 +846,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--stencil", type=int, nargs=4, default=None, help="time one stencil variant on this lattice")
-    ap.add_argument("--variant", type=int, default=2, help="0 hop, 1 hop+A^-1, 2 hop+A^-1+xpay+out2+norm, 3 the CG update stencil (D^dag, xpay, x and r update, norm)")
+    ap.add_argument("--variant", type=int, default=2, help="0 hop, 1 hop+A^-1, 2 hop+A^-1+xpay+out2+norm, 3 the CG update stencil (D^dag, xpay, x and r update, norm), 4 variant 2 without the norm")
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--sb", type=int, default=0, help="site lanes per block for --stencil (0 = library default)")

@@ -242,7 +242,9 @@ void* qcuHostAlloc(long long bytes);
 void qcuHostFree(void* p);
 
 /* Times the fused stencil kernel on resident internal fields: `variant`
- * 0 = hop only, 1 = hop + A^-1, 2 = hop + A^-1 + xpay; precision as above;
+ * 0 = hop only, 1 = hop + A^-1, 2 = hop + A^-1 + xpay + second output + norm
+ * (the CG's K2), 3 = the CG update stencil, 4 = variant 2 without the norm
+ * and its reduction; precision as above;
  * nrhs right-hand sides. Runs `iters` launches and returns the mean device
  * time per launch in milliseconds, measured with CUDA events on the
  * context stream; *bytes receives the algorithmic bytes of one launch. */

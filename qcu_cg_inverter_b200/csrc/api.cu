@@ -119,11 +119,16 @@ int Scratch::ensure(const Geom& g, int nrhs, cudaStream_t st, int min_sb) {
   // partials: one per (rhs, quantity <= 2, block) for up to 2*Vh_pad sites
   // (full-spinor dot products) in blocks of at least min_sb site lanes
   if (min_sb < 1) min_sb = 1;
-  size_t need = (size_t)((g.Vh_pad * 2 + min_sb - 1) / min_sb + 1) * (size_t)nrhs * 2;
+  const size_t tiles = (size_t)((g.Vh_pad * 2 + min_sb - 1) / min_sb + 1);
+  const size_t groups = (tiles + kReduceGroup - 1) / kReduceGroup + 1;
+  size_t need = tiles * (size_t)nrhs * 2;
   if (need > partial_doubles || !partial.p) {
     QCU_CHECK(partial.ensure(need * sizeof(double), st));
     partial_doubles = need;
   }
+  // second-level partials and the groups' counters (RHS tiles <= nrhs)
+  QCU_CHECK(partial2.ensure(groups * (size_t)nrhs * 2 * sizeof(double), st));
+  QCU_CHECK(group_ticket.ensure(groups * (size_t)nrhs * sizeof(unsigned), st));
   QCU_CHECK(ticket.ensure(64, st));
   QCU_CHECK(result.ensure((size_t)nrhs * 2 * sizeof(double) + 64, st));
   QCU_CHECK(host.ensure((size_t)nrhs * 2 * sizeof(double) + 64));

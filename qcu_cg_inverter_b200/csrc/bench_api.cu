@@ -53,7 +53,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
                                double* bytes) {
   clear_error();
   QCU_CHECK(ctx_check(ctx));
-  if (prec < 0 || prec > 2 || variant < 0 || variant > 3 || nrhs < 1 || iters < 1) {
+  if (prec < 0 || prec > 2 || variant < 0 || variant > 4 || nrhs < 1 || iters < 1) {
     set_error(QCU_ERR_INVALID_ARG, "bad benchmark arguments");
     return QCU_ERR_INVALID_ARG;
   }
@@ -99,7 +99,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
     QCU_CHECK_CUDA(cudaStreamSynchronize(st));
   }
   int slot = 0;
-  if (variant == 1 || variant == 2) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
+  if (variant == 1 || variant == 2 || variant == 4) QCU_CHECK(ctx_clover_slot(ctx, 0.13, &slot));
   // the shape the solver would use (tuned when qcuAutotune ran, else the
   // default), unless qcuContextSetShape overrode the single-RHS shape
   LaunchShape sh = (nrhs == 1 && ctx->shape_set) ? ctx->shape1 : ctx_shape(ctx, op, nrhs);
@@ -127,6 +127,7 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   const int epi = variant == 0   ? 0
                   : variant == 1 ? EPI_CPRE
                   : variant == 2 ? (EPI_CPRE | EPI_XPAY | EPI_OUT2 | EPI_NORM)
+                  : variant == 4 ? (EPI_CPRE | EPI_XPAY | EPI_OUT2)
                                  : (EPI_XPAY | EPI_CGXR);
   const bool dag = variant == 3;  // the CG update stencil applies D^dag
   for (int k = 0; k < 3; k++) QCU_CHECK_CUDA(launch_dslash(op, dag, epi, FIN_NONE, a, sh, st));
@@ -145,9 +146,10 @@ extern "C" int qcuBenchStencil(qcu_context ctx, int prec, int variant, int nrhs,
   if (ms_per_launch) *ms_per_launch = (double)ms / iters;
   if (bytes) {
     double per_rhs = 8.0 * spinor_b(prec) + spinor_b(prec);
-    if (variant == 2) per_rhs += 2.0 * spinor_b(prec);  // xpay input + second output
+    if (variant == 2 || variant == 4) per_rhs += 2.0 * spinor_b(prec);  // xpay input + second output
     if (variant == 3) per_rhs += 2.0 * spinor_b(prec) - spinor_b(prec) + 4.0 * spinor_b(pa);  // x, p in; no out; x, r in and out
-    double shared = 8.0 * link_b(op_link_format(op)) + ((variant == 1 || variant == 2) ? clov_b(op_clover_prec(op)) : 0.0);
+    double shared = 8.0 * link_b(op_link_format(op)) +
+                    ((variant == 1 || variant == 2 || variant == 4) ? clov_b(op_clover_prec(op)) : 0.0);
     int tiles = (nrhs + sh.Rb - 1) / sh.Rb;
     *bytes = (double)g.Vh * (nrhs * per_rhs + tiles * shared);
   }

@@ -108,13 +108,14 @@ struct CloverBank {
 };
 
 struct Scratch {
-  DevBuf partial, ticket, result;
+  DevBuf partial, ticket, result, partial2, group_ticket;
   PinnedBuf host;
   size_t partial_doubles = 0;
   // min_sb: the fewest site lanes per block of any launch that reduces
   int ensure(const Geom& g, int nrhs, cudaStream_t st, int min_sb);
   ReduceArgs args(void* state = nullptr) const {
-    return ReduceArgs{partial.as<double>(), ticket.as<unsigned>(), result.as<double>(), state};
+    return ReduceArgs{partial.as<double>(), ticket.as<unsigned>(), result.as<double>(), state,
+                      partial2.as<double>(), group_ticket.as<unsigned>()};
   }
 };
 

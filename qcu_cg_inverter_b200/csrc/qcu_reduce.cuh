@@ -3,21 +3,24 @@
 // Kernels run with a 2-D thread block: threadIdx.x = right-hand side within the
 // block's RHS tile (Rb lanes), threadIdx.y = site. Each block reduces its
 // per-RHS values with warp shuffles (over the site lanes only) and shared
-// memory, writes one partial per (rhs, quantity), and the last block to finish
-// (atomic ticket) sums the partials in a fixed order and calls a finishing
+// memory and writes one partial per (rhs, quantity). The last block of each
+// group of site tiles (atomic counters) sums the group's partials, and the
+// last group sums the group sums, in a fixed order, and calls a finishing
 // functor with the totals. The result therefore depends only on the launch
-// shape, never on timing. Partials and tickets live in caller-provided scratch
-// memory; the last block re-arms the ticket to 0.
+// shape, never on timing. Partials and counters live in caller-provided
+// scratch memory; the blocks that finish re-arm the counters to 0.
 #pragma once
 #include "qcu_common.cuh"
 
 namespace qcu {
 
 struct ReduceArgs {
-  double* partial;      // [nrhs*NR][gridDim.x] doubles
-  unsigned* ticket;     // one counter, 0 on entry
-  double* result;       // [nrhs*NR] totals (written by the last block)
-  void* state;          // passed to the finishing functor
+  double* partial;         // [nrhs*NR][site tiles] doubles
+  unsigned* ticket;        // one counter, 0 on entry
+  double* result;          // [nrhs*NR] totals (written by the last block)
+  void* state;             // passed to the finishing functor
+  double* partial2;        // [nrhs*NR][site-tile groups] doubles
+  unsigned* group_ticket;  // [site-tile groups][RHS tiles] counters, 0 on entry
 };
 
 // No finishing step: totals are left in result[].
@@ -43,9 +46,28 @@ struct TileCoord {
   }
 };
 
+// Site tiles per group of the two-level finish: the last block of each group
+// (per RHS tile) sums the group's partials into one second-level partial, and
+// the last group to finish sums those and applies the functor.
+constexpr int kReduceGroup = 128;
+// Reductions of fewer partials (RHS x quantities x site tiles) than this keep
+// the one-level finish: for them the second level's extra barrier, fence and
+// counter on the last block's path cost more than its shorter sum (measured on
+// B200: 16^3x32 single-RHS K2 14.6 us one-level, 16.4 us two-level)
+constexpr size_t kTwoLevelMin = 4096;
+
 // vals: NR values for each of the RL right-hand sides of this thread (RHS
 // (t.rhs*Rb + threadIdx.x)*RL + j holds vals[j*NR .. j*NR+NR-1]; zero for idle
 // threads). Every thread of the block must call this.
+//
+// Two-level finish (reductions of at least kTwoLevelMin partials): with one
+// serial last block the final sum ran over every site tile (10368 per RHS at
+// 24^3x48) on one SM while the GPU idled (measured on B200: the norm and its
+// reduction cost the fused K2 0.33 of 1.95 ms with 48 RHS). Groups of
+// kReduceGroup site tiles are summed by their last block as the launch runs;
+// the last group then sums ceil(nsite / kReduceGroup) values per quantity
+// (K2 with 48 RHS: 1.95 -> 1.79 ms). The order of every sum is fixed by the
+// tile numbering, so the result still depends only on the launch shape.
 template <int NR, class Fin, int RL = 1>
 QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs& red,
                                const TileCoord t = TileCoord::from_grid()) {
@@ -75,22 +97,79 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
       }
     }
   }
-  __threadfence();
+  // The block counts once its partials are visible: after the barrier, thread
+  // 0's fence orders every thread's stores before the counter (fences are
+  // cumulative over the barrier, as in a release by one thread of the block).
   __syncthreads();
+  if ((size_t)nrhs * NR * t.nsite < kTwoLevelMin) {
+    // one level: the last block of the launch sums every partial
+    if (tid == 0) {
+      __threadfence();
+      const unsigned c = atomicAdd(red.ticket, 1u);
+      am_last = (c == t.nblocks - 1u);
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    const int nq = nrhs * NR;
+    for (int q = warp; q < nq; q += nwarps) {
+      double acc = 0.0;
+      const volatile double* p = red.partial + (size_t)q * t.nsite;
+      for (int b = lane; b < t.nsite; b += 32) acc += p[b];
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) red.result[q] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      Fin::apply(red.result, nrhs, NR, red.state);
+      __threadfence();
+      *red.ticket = 0u;
+    }
+    return;
+  }
+  // two levels: the block's arrival in its group
+  const int ntiles = (int)(t.nblocks / (unsigned)t.nsite);  // RHS tiles
+  const int ngroups = (t.nsite + kReduceGroup - 1) / kReduceGroup;
+  const int g = t.site / kReduceGroup;
+  const int g0 = g * kReduceGroup, g1 = min(g0 + kReduceGroup, t.nsite);
   if (tid == 0) {
-    const unsigned total = t.nblocks;
-    unsigned t = atomicAdd(red.ticket, 1u);
-    am_last = (t == total - 1);
+    __threadfence();
+    const unsigned c = atomicAdd(red.group_ticket + (size_t)g * ntiles + t.rhs, 1u);
+    am_last = (c == (unsigned)(g1 - g0) - 1u);
   }
   __syncthreads();
   if (!am_last) return;
   __threadfence();
-  // last block: one warp per (rhs, quantity), lanes stride over the blocks
+  // last block of the group: its RHS tile's quantities, one warp each, lanes
+  // over the group's site tiles
+  {
+    const int r0 = t.rhs * Rb * RL;
+    const int nloc = max(0, min(Rb * RL, nrhs - r0)) * NR;
+    for (int ql = warp; ql < nloc; ql += nwarps) {
+      const int q = r0 * NR + ql;
+      double acc = 0.0;
+      const volatile double* p = red.partial + (size_t)q * t.nsite;
+      for (int b = g0 + lane; b < g1; b += 32) acc += p[b];
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) red.partial2[(size_t)q * ngroups + g] = acc;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    red.group_ticket[(size_t)g * ntiles + t.rhs] = 0u;  // every member has arrived
+    __threadfence();  // the group's sums are visible before the group counts
+    const unsigned c = atomicAdd(red.ticket, 1u);
+    am_last = (c == (unsigned)(ngroups * ntiles) - 1u);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  // last group: one warp per (rhs, quantity), lanes over the groups
   const int nq = nrhs * NR;
   for (int q = warp; q < nq; q += nwarps) {
     double acc = 0.0;
-    const volatile double* p = red.partial + (size_t)q * t.nsite;
-    for (int b = lane; b < t.nsite; b += 32) acc += p[b];
+    const volatile double* p = red.partial2 + (size_t)q * ngroups;
+    for (int b = lane; b < ngroups; b += 32) acc += p[b];
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (lane == 0) red.result[q] = acc;
   }
