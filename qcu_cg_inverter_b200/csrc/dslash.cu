@@ -2,6 +2,7 @@
 // dslash_f64.cu, dslash_f32.cu and dslash_f16.cu).
 #include <stdlib.h>
 
+#include "qcu_cg_state.cuh"
 #include "qcu_kernels.cuh"
 
 namespace qcu {
@@ -94,7 +95,8 @@ cudaError_t prepare_staged_kernels() {
 }
 
 cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape sh,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, int* launched) {
+  if (launched) *launched = 0;
   const bool pairs = g_pairs_override < 0 ? QCU_RHS_PAIRS != 0 : g_pairs_override != 0;
   const bool pair_cgxr = g_pairs_override < 0 ? QCU_PAIR_CGXR != 0 : g_pairs_override != 0;
   DslashKernelFn fn = nullptr;
@@ -129,16 +131,31 @@ cudaError_t launch_dslash(int prec, bool dagger, int epi, int fin, const DslashA
   const int nsites = (a.s_lim > 0 ? a.s_lim : a.g.Vh) - a.s_off;
   if (nsites <= 0) return cudaSuccess;
 
+  // a reduction over this launch's site tiles alone, large enough to defer
+  const int site_tiles = grid_x(nsites, sh.Sb);
+  const bool reduces = (epi & (EPI_NORM | EPI_CGXR)) != 0;
+  const bool defer = reduces && a.block_total == 0 && (size_t)a.nrhs * site_tiles >= kTwoLevelMin;
+  DslashArgs b = a;
+  b.red.deferred = defer ? 1 : 0;
   if (QCU_SLAB_MINOR && nslab > 1) {
     // the RHS tiles of one site tile run back to back, so its links and
     // clover are read from DRAM once and served from L2 to the others
-    DslashArgs b = a;
     b.nslab = nslab;
-    fn<<<dim3(grid_x(nsites, sh.Sb) * nslab, 1), block, smem, stream>>>(b);
+    fn<<<dim3(site_tiles * nslab, 1), block, smem, stream>>>(b);
   } else {
-    DslashArgs b = a;
     b.nslab = 0;
-    fn<<<dim3(grid_x(nsites, sh.Sb), nslab), block, smem, stream>>>(b);
+    fn<<<dim3(site_tiles, nslab), block, smem, stream>>>(b);
+  }
+  if (launched) *launched = 1;
+  if (defer) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    switch (fin) {
+      case FIN_CG_ALPHA: reduce_finish_kernel<FinCgAlpha><<<a.nrhs, 256, 0, stream>>>(b.red, site_tiles, a.nrhs, 1); break;
+      case FIN_CG_BETA: reduce_finish_kernel<FinCgBeta><<<a.nrhs, 256, 0, stream>>>(b.red, site_tiles, a.nrhs, 1); break;
+      default: reduce_finish_kernel<FinNone><<<a.nrhs, 256, 0, stream>>>(b.red, site_tiles, a.nrhs, 1); break;
+    }
+    if (launched) *launched = 2;
   }
   return cudaGetLastError();
 }

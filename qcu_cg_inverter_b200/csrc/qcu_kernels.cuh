@@ -76,8 +76,11 @@ struct LaunchShape {
 
 // `op` is an OpVariant (spinor / link / clover storage); the pointers in `a`
 // must be fields of those formats.
+// A reduction of at least kTwoLevelMin partials (and not shared with other
+// launches) is deferred: the stencil only writes its partials and a finishing
+// launch follows. *launched (if given) receives the number of kernels launched.
 cudaError_t launch_dslash(int op, bool dagger, int epi, int fin, const DslashArgs& a, LaunchShape shape,
-                          cudaStream_t stream);
+                          cudaStream_t stream, int* launched = nullptr);
 // Test hook: batched launches of the fast 16-bit operator on the RHS-paired
 // kernels for every epilogue (1), on one RHS per thread (0), or as built (-1).
 void set_rhs_pairs_override(int v);

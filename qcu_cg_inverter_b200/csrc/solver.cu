@@ -191,16 +191,19 @@ DslashArgs op_args(const OpCtx& o, int prec, int parity, const Field& in, const 
 
 int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& a) {
   if (!o.ctx->g.tdd) {
-    QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, fin, a, o.w->shape, o.st));
-    o.ctx->launches++;
+    int n = 0;
+    QCU_CHECK_CUDA(launch_dslash(prec, dag, epi, fin, a, o.w->shape, o.st, &n));
+    o.ctx->launches += n;
     return QCU_SUCCESS;
   }
   // a t-slab: the input's ghost slices from the neighbouring ranks first; the
   // per-RHS sums of the launch are this slab's part, summed over the ranks
   // before the finishing functor runs
   QCU_CHECK(dd_stencil(o.ctx, a, op_spinor_prec(prec), o.w->shape, o.st, [&](const DslashArgs& piece) {
-    o.ctx->launches++;
-    return launch_dslash(prec, dag, epi, FIN_NONE, piece, o.w->shape, o.st);
+    int n = 0;
+    const cudaError_t e = launch_dslash(prec, dag, epi, FIN_NONE, piece, o.w->shape, o.st, &n);
+    o.ctx->launches += n;
+    return e;
   }));
   if (epi & (EPI_NORM | EPI_CGXR)) {
     QCU_CHECK(dd_sum(o.ctx, a.red.result, a.nrhs, o.st));
