@@ -270,11 +270,15 @@ int ctx_clover_slot(qcu_context ctx, double csw_eff, int* slot, bool wait) {
   }
   QCU_CHECK(ctx->status.ensure(64, ctx->stream));
   QCU_CHECK_CUDA(cudaMemsetAsync(ctx->status.p, 0, 64, ctx->stream));
+  QCU_CHECK(B.F64.ensure(B.b64, ctx->stream));
+  const bool F_ready = B.F_version == ctx->gauge_version;
   QCU_CHECK_CUDA(launch_clover_build(ctx->g, ctx->gauge64.p, csw_eff, static_cast<char*>(B.A64.p) + B.b64 * k,
                                      static_cast<char*>(B.Ainv64.p) + B.b64 * k,
                                      static_cast<char*>(B.Ainv32.p) + B.b32 * k,
-                                     static_cast<char*>(B.Ainv16.p) + B.b16 * k, ctx->status.as<int>(), ctx->stream));
-  ctx->launches += 2;
+                                     static_cast<char*>(B.Ainv16.p) + B.b16 * k, ctx->status.as<int>(), ctx->stream,
+                                     B.F64.p, F_ready));
+  B.F_version = ctx->gauge_version;
+  ctx->launches += F_ready ? 2 : 3;
   if (!wait) {
     B.csw[k] = csw_eff;
     B.stamp[k] = ++ctx->clock;
@@ -601,7 +605,8 @@ long long qcuContextDeviceBytes(qcu_context ctx) {
   if (!ctx) return 0;
   long long n = ctx->gauge64.bytes + ctx->gauge32.bytes + ctx->gauge16.bytes + ctx->gauge18.bytes;
   n += qcu_engine_device_bytes(ctx);
-  n += ctx->clover.A64.bytes + ctx->clover.Ainv64.bytes + ctx->clover.Ainv32.bytes + ctx->clover.Ainv16.bytes;
+  n += ctx->clover.A64.bytes + ctx->clover.Ainv64.bytes + ctx->clover.Ainv32.bytes + ctx->clover.Ainv16.bytes +
+       ctx->clover.F64.bytes;
   n += ctx->red.partial.bytes + ctx->lin.data.bytes + ctx->lout.data.bytes + ctx->ltmp.data.bytes +
        ctx->ltmp2.data.bytes + ctx->lx.data.bytes + ctx->stage_in.bytes + ctx->stage_out.bytes;
   return n;

@@ -102,6 +102,8 @@ struct CloverBank {
   int capacity = 0;
   size_t b64 = 0, b32 = 0, b16 = 0;
   DevBuf A64, Ainv64, Ainv32, Ainv16;
+  DevBuf F64;                     // the kappa-independent field term of the current links
+  long long F_version = -1;       // gauge_version F64 belongs to
   std::vector<double> csw;       // csw_eff of each slot (NaN = free)
   std::vector<long long> stamp;  // last use, for eviction
   std::vector<int> pinned;       // slots used by the batch being prepared
@@ -247,8 +249,11 @@ int ingest_gauge(qcu_context ctx, const void* gauge);
 // seeded field of the global lattice restricted to the slab
 int dd_ingest_gauge(qcu_context ctx, const void* gauge);
 int dd_generate_gauge(qcu_context ctx, uint64_t seed, double eps);
+// A = 1 + csw_eff F and its inverse into the given fields; F (the
+// kappa-independent field term, one packed FP64 field) is built from the links
+// first unless F_ready
 cudaError_t launch_clover_build(const Geom& g, const void* gauge64, double csw_eff, void* A64, void* Ainv64,
-                                void* Ainv32, void* Ainv16, int* status, cudaStream_t stream);
+                                void* Ainv32, void* Ainv16, int* status, cudaStream_t stream, void* F64, bool F_ready);
 cudaError_t launch_clover_apply(int prec, const Geom& g, int parity, int nrhs, CSpinorView in, SpinorView out,
                                 const void* clov, size_t clov_stride, const int* clov_idx, const int* active,
                                 const ReduceArgs* red, LaunchShape sh, cudaStream_t stream);

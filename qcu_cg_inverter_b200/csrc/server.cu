@@ -92,6 +92,7 @@ long long resident_estimate(const qcu_server_params& P, const int L[4]) {
   const long long c16 = (clover_field_bytes(PREC_HALF, vp) + 255) & ~(size_t)255;
   n += (long long)P.clover_slots *
        (2 * (long long)clover_field_bytes(PREC_DOUBLE, vp) + (long long)clover_field_bytes(PREC_SINGLE, vp) + c16);
+  n += (long long)clover_field_bytes(PREC_DOUBLE, vp);  // the kappa-independent field term
   const int ps = P.precision, pa = ps == PREC_DOUBLE ? PREC_DOUBLE : PREC_SINGLE;
   n += 9LL * spinor_field_bytes(PREC_DOUBLE, vp, cap);  // b (2 parities), bhat, x, x_o, 4 FP64 temporaries
   n += 2LL * spinor_field_bytes(pa, vp, cap);
