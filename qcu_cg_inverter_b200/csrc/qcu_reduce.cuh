@@ -59,6 +59,36 @@ constexpr int kReduceGroup = 128;
 // B200: 16^3x32 single-RHS K2 14.6 us one-level, 16.4 us two-level)
 constexpr size_t kTwoLevelMin = 4096;
 
+// Sums p[b0], p[b0 + step], ... (indices below n) in that order. The loads
+// bypass L1 (the partials were stored by other blocks of the launch) and eight
+// are in flight at once; the adds keep the sequential order, so the total is
+// the same as a plain loop's.
+QCU_D double strided_sum(const double* p, int b0, int n, int step) {
+  double acc = 0.0;
+  int b = b0;
+  for (; b + 7 * step < n; b += 8 * step) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = __ldcg(p + b + k * step);
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc += v[k];
+  }
+  for (; b < n; b += step) acc += __ldcg(p + b);
+  return acc;
+}
+
+// Adds one to a counter at GPU scope with acquire-release semantics. Called by
+// thread 0 after a block barrier, the release covers every store the block
+// made before the barrier (fences are cumulative), and the block that reads
+// the final count sees all of the counted blocks' stores once it has passed
+// its own barrier after this call. Cheaper than a sequentially consistent
+// fence (__threadfence) followed by a relaxed atomic.
+QCU_D unsigned ticket_arrive(unsigned* p) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 // vals: NR values for each of the RL right-hand sides of this thread (RHS
 // (t.rhs*Rb + threadIdx.x)*RL + j holds vals[j*NR .. j*NR+NR-1]; zero for idle
 // threads). Every thread of the block must call this.
@@ -107,26 +137,19 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   __syncthreads();
   if ((size_t)nrhs * NR * t.nsite < kTwoLevelMin) {
     // one level: the last block of the launch sums every partial
-    if (tid == 0) {
-      __threadfence();
-      const unsigned c = atomicAdd(red.ticket, 1u);
-      am_last = (c == t.nblocks - 1u);
-    }
+    if (tid == 0) am_last = (ticket_arrive(red.ticket) == t.nblocks - 1u);
     __syncthreads();
     if (!am_last) return;
-    __threadfence();
     const int nq = nrhs * NR;
     for (int q = warp; q < nq; q += nwarps) {
-      double acc = 0.0;
-      const volatile double* p = red.partial + (size_t)q * t.nsite;
-      for (int b = lane; b < t.nsite; b += 32) acc += p[b];
+      double acc = strided_sum(red.partial + (size_t)q * t.nsite, lane, t.nsite, 32);
       for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
       if (lane == 0) red.result[q] = acc;
     }
     __syncthreads();
     if (tid == 0) {
+      // the next launch that uses the counter sees the reset (launch boundary)
       Fin::apply(red.result, nrhs, NR, red.state);
-      __threadfence();
       *red.ticket = 0u;
     }
     return;
@@ -136,14 +159,9 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   const int ngroups = (t.nsite + kReduceGroup - 1) / kReduceGroup;
   const int g = t.site / kReduceGroup;
   const int g0 = g * kReduceGroup, g1 = min(g0 + kReduceGroup, t.nsite);
-  if (tid == 0) {
-    __threadfence();
-    const unsigned c = atomicAdd(red.group_ticket + (size_t)g * ntiles + t.rhs, 1u);
-    am_last = (c == (unsigned)(g1 - g0) - 1u);
-  }
+  if (tid == 0) am_last = (ticket_arrive(red.group_ticket + (size_t)g * ntiles + t.rhs) == (unsigned)(g1 - g0) - 1u);
   __syncthreads();
   if (!am_last) return;
-  __threadfence();
   // last block of the group: its RHS tile's quantities, one warp each, lanes
   // over the group's site tiles
   {
@@ -151,9 +169,7 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
     const int nloc = max(0, min(Rb * RL, nrhs - r0)) * NR;
     for (int ql = warp; ql < nloc; ql += nwarps) {
       const int q = r0 * NR + ql;
-      double acc = 0.0;
-      const volatile double* p = red.partial + (size_t)q * t.nsite;
-      for (int b = g0 + lane; b < g1; b += 32) acc += p[b];
+      double acc = strided_sum(red.partial + (size_t)q * t.nsite, g0 + lane, g1, 32);
       for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
       if (lane == 0) red.partial2[(size_t)q * ngroups + g] = acc;
     }
@@ -161,26 +177,21 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
   __syncthreads();
   if (tid == 0) {
     red.group_ticket[(size_t)g * ntiles + t.rhs] = 0u;  // every member has arrived
-    __threadfence();  // the group's sums are visible before the group counts
-    const unsigned c = atomicAdd(red.ticket, 1u);
-    am_last = (c == (unsigned)(ngroups * ntiles) - 1u);
+    // the release makes the group's sums visible before the group counts
+    am_last = (ticket_arrive(red.ticket) == (unsigned)(ngroups * ntiles) - 1u);
   }
   __syncthreads();
   if (!am_last) return;
-  __threadfence();
   // last group: one warp per (rhs, quantity), lanes over the groups
   const int nq = nrhs * NR;
   for (int q = warp; q < nq; q += nwarps) {
-    double acc = 0.0;
-    const volatile double* p = red.partial2 + (size_t)q * ngroups;
-    for (int b = lane; b < ngroups; b += 32) acc += p[b];
+    double acc = strided_sum(red.partial2 + (size_t)q * ngroups, lane, ngroups, 32);
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if (lane == 0) red.result[q] = acc;
   }
   __syncthreads();
   if (tid == 0) {
     Fin::apply(red.result, nrhs, NR, red.state);
-    __threadfence();
     *red.ticket = 0u;
   }
 }
@@ -198,9 +209,7 @@ __global__ void __launch_bounds__(256) reduce_finish_kernel(ReduceArgs red, int 
   __shared__ bool am_last;
   const int q = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
-  double acc = 0.0;
-  const double* p = red.partial + (size_t)q * nsite;
-  for (int b = tid; b < nsite; b += blockDim.x) acc += p[b];
+  double acc = strided_sum(red.partial + (size_t)q * nsite, tid, nsite, blockDim.x);
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) sm[warp] = acc;
   __syncthreads();
@@ -208,15 +217,11 @@ __global__ void __launch_bounds__(256) reduce_finish_kernel(ReduceArgs red, int 
     double s = 0.0;
     for (int w = 0; w < nwarps; w++) s += sm[w];
     red.result[q] = s;
-    __threadfence();
-    const unsigned c = atomicAdd(red.ticket, 1u);
-    am_last = (c == gridDim.x - 1u);
+    am_last = (ticket_arrive(red.ticket) == gridDim.x - 1u);
   }
   __syncthreads();
   if (!am_last || tid != 0) return;
-  __threadfence();
   Fin::apply(red.result, nrhs, NR, red.state);
-  __threadfence();
   *red.ticket = 0u;
 }
 
