@@ -1,6 +1,7 @@
 // Device-resident CG scalars, one entry per right-hand side, and the finishing
-// functors that update them at the end of a fused reduction (executed by one
-// thread of the last block, so no host round trip is needed per iteration).
+// functors that update them at the end of a fused reduction (executed by every
+// thread of the last block, thread t of nt for RHS t, t + nt, ..., so no host
+// round trip is needed per iteration and no thread walks all the RHS).
 //
 // Iteration of the sloppy CG on N = Mhat^dag Mhat (per RHS r):
 //   y = Mhat p, pAp = |y|^2           -> FinCgAlpha: alpha = rr / pAp
@@ -36,10 +37,12 @@ struct CgDevState {
   double align;
 };
 
+// Every thread of the block calls apply (t = its index, nt = the block's
+// threads): FinCgBeta has a block barrier.
 struct FinCgAlpha {
-  static QCU_D void apply(const double* res, int nrhs, int NR, void* st) {
+  static QCU_D void apply(const double* res, int nrhs, int NR, void* st, int t, int nt) {
     CgDevState* s = static_cast<CgDevState*>(st);
-    for (int r = 0; r < nrhs; r++) {
+    for (int r = t; r < nrhs; r += nt) {
       if (!s->active[r]) continue;
       double pap = res[r * NR];
       s->pAp[r] = pap;
@@ -56,10 +59,10 @@ struct FinCgAlpha {
 };
 
 struct FinCgBeta {
-  static QCU_D void apply(const double* res, int nrhs, int NR, void* st) {
+  static QCU_D void apply(const double* res, int nrhs, int NR, void* st, int t, int nt) {
     CgDevState* s = static_cast<CgDevState*>(st);
     bool paused = false;
-    for (int r = 0; r < nrhs; r++) {
+    for (int r = t; r < nrhs; r += nt) {
       if (!s->active[r]) continue;
       double rn = res[r * NR];
       s->beta[r] = rn / s->rr[r];
@@ -76,8 +79,10 @@ struct FinCgBeta {
         paused = true;
       }
     }
-    if (paused && s->align > 1.0) {
-      for (int r = 0; r < nrhs; r++) {
+    // a thread reads back only its own RHS below: the barrier only has to
+    // tell every thread whether any RHS paused
+    if (__syncthreads_or(paused) && s->align > 1.0) {
+      for (int r = t; r < nrhs; r += nt) {
         if (s->active[r] && !s->final_trig[r] && s->rr[r] < s->align * s->trigger[r]) {
           s->active[r] = 0;
           s->event[r] = 1;

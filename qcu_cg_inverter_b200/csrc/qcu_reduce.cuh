@@ -28,7 +28,7 @@ struct ReduceArgs {
 
 // No finishing step: totals are left in result[].
 struct FinNone {
-  static QCU_D void apply(const double*, int, int, void*) {}
+  static QCU_D void apply(const double*, int, int, void*, int, int) {}
 };
 
 // every reducing kernel is launched with at most 256 threads (its
@@ -147,11 +147,9 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
       if (lane == 0) red.result[q] = acc;
     }
     __syncthreads();
-    if (tid == 0) {
-      // the next launch that uses the counter sees the reset (launch boundary)
-      Fin::apply(red.result, nrhs, NR, red.state);
-      *red.ticket = 0u;
-    }
+    Fin::apply(red.result, nrhs, NR, red.state, tid, nthreads);
+    // the next launch that uses the counter sees the reset (launch boundary)
+    if (tid == 0) *red.ticket = 0u;
     return;
   }
   // two levels: the block's arrival in its group
@@ -190,10 +188,8 @@ QCU_D void block_reduce_finish(double vals[NR * RL], int nrhs, const ReduceArgs&
     if (lane == 0) red.result[q] = acc;
   }
   __syncthreads();
-  if (tid == 0) {
-    Fin::apply(red.result, nrhs, NR, red.state);
-    *red.ticket = 0u;
-  }
+  Fin::apply(red.result, nrhs, NR, red.state, tid, nthreads);
+  if (tid == 0) *red.ticket = 0u;
 }
 
 // The finishing launch of a deferred reduction: block q sums quantity q's
@@ -220,9 +216,9 @@ __global__ void __launch_bounds__(256) reduce_finish_kernel(ReduceArgs red, int 
     am_last = (ticket_arrive(red.ticket) == gridDim.x - 1u);
   }
   __syncthreads();
-  if (!am_last || tid != 0) return;
-  Fin::apply(red.result, nrhs, NR, red.state);
-  *red.ticket = 0u;
+  if (!am_last) return;
+  Fin::apply(red.result, nrhs, NR, red.state, tid, (int)blockDim.x);
+  if (tid == 0) *red.ticket = 0u;
 }
 
 }  // namespace qcu

@@ -217,12 +217,12 @@ int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& 
 
 template <class Fin>
 __global__ void fin_kernel(const ReduceArgs red, int nrhs) {
-  Fin::apply(red.result, nrhs, 1, red.state);
+  Fin::apply(red.result, nrhs, 1, red.state, (int)threadIdx.x, (int)blockDim.x);
 }
 
 cudaError_t launch_fin(int fin, const ReduceArgs& red, int nrhs, cudaStream_t st) {
-  if (fin == FIN_CG_ALPHA) fin_kernel<FinCgAlpha><<<1, 1, 0, st>>>(red, nrhs);
-  else if (fin == FIN_CG_BETA) fin_kernel<FinCgBeta><<<1, 1, 0, st>>>(red, nrhs);
+  if (fin == FIN_CG_ALPHA) fin_kernel<FinCgAlpha><<<1, 64, 0, st>>>(red, nrhs);
+  else if (fin == FIN_CG_BETA) fin_kernel<FinCgBeta><<<1, 64, 0, st>>>(red, nrhs);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
