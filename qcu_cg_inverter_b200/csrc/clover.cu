@@ -14,6 +14,7 @@
 // Kernel shape: a block handles 32 sites; thread (plane, site) computes the
 // six G_munu into shared memory, then thread (block b, site) assembles chiral
 // block b, factors it and writes A and A^-1.
+#include "qcu_cg_state.cuh"
 #include "qcu_fields.cuh"
 #include "qcu_kernels.cuh"
 
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(256) clover_apply_kernel(Geom g, int parity, i
 // r, one 6x6 block of A, then of A^-1), so a thread holds one block and half a
 // spinor. PU = the sloppy precision: u and r rounded to it (the inputs of the
 // sloppy-operator r_ne), with the roundings of a separate conversion.
-template <int PU>
+template <int PU, class Fin>
 __global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, int nrhs, CSpinorView rin, SpinorView u,
                                                             SpinorView rs, const void* A, const void* Ainv,
                                                             size_t clov_stride, const int* clov_idx, const int* active,
@@ -412,15 +413,23 @@ __global__ void __launch_bounds__(256, 2) clover_res_kernel(Geom g, int parity, 
     }
   }
   double vv[1] = {nrm};
-  block_reduce_finish<1, FinNone>(vv, nrhs, red);
+  block_reduce_finish<1, Fin>(vv, nrhs, red);
 }
 
 cudaError_t launch_clover_res(int pu, const Geom& g, int parity, int nrhs, CSpinorView r, SpinorView u, SpinorView rs,
                               const void* A, const void* Ainv, size_t clov_stride, const int* clov_idx,
-                              const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t stream) {
+                              const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t stream,
+                              int fin) {
   dim3 block(sh.Rb, sh.Sb);
   dim3 grid(grid_x(g.Vh, sh.Sb), (nrhs + sh.Rb - 1) / sh.Rb);
-#define QCU_CR(P) clover_res_kernel<P><<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, rs, A, Ainv, clov_stride, clov_idx, active, red)
+  if (fin != FIN_NONE && (fin != FIN_REL_CONT || !red.state)) return cudaErrorInvalidValue;
+#define QCU_CR(P)                                                                                                   \
+  if (fin == FIN_REL_CONT)                                                                                          \
+    clover_res_kernel<P, FinRelCont><<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, rs, A, Ainv, clov_stride,   \
+                                                                 clov_idx, active, red);                            \
+  else                                                                                                              \
+    clover_res_kernel<P, FinNone><<<grid, block, 0, stream>>>(g, parity, nrhs, r, u, rs, A, Ainv, clov_stride,      \
+                                                              clov_idx, active, red)
   switch (pu) {
     case PREC_DOUBLE: QCU_CR(PREC_DOUBLE); break;
     case PREC_SINGLE: QCU_CR(PREC_SINGLE); break;

@@ -120,6 +120,7 @@ int Engine::configure(qcu_context c, int cap_, const EngineParams& p) {
   if (!step_ev) QCU_CHECK_CUDA(cudaEventCreateWithFlags(&step_ev, cudaEventDisableTiming));
   const double delta = (P.delta > 0 && P.delta < 1) ? P.delta : default_delta(P.precision);
   rp_ = RelParams{P.tol, delta * delta, P.maxiter, P.clover ? 1 : 0};
+  QCU_CHECK(ws_set_stop(ctx, w, P.tol, P.maxiter));
   const double sig[5] = {P.bc_t, P.tol, delta * delta, (double)P.maxiter, P.clover ? 1.0 : 0.0};
   if (memcmp(sig, w.graph_sig, sizeof(sig)) != 0) {
     w.drop_graphs();
@@ -426,8 +427,10 @@ int Engine::observe(std::vector<Group*>* retired) {
       rep.kappa = q->kappa;
       {
         const int share = cap > 1 ? w.shape.Rb : 1;  // RHS served by one link / clover load
+        // the last reliable update stopped the column: it computed no r_ne
         const double per_site = rep.iterations * iteration_bytes(w.op, P.clover, share) +
-                                rep.reliable_updates * reliable_update_bytes(w.op, P.clover, share) +
+                                rep.reliable_updates * reliable_update_bytes(w.op, P.clover, share) -
+                                (rep.reliable_updates > 0 ? reliable_update_ne_bytes(w.op, P.clover, share) : 0.0) +
                                 admit_retire_bytes(P.clover, share);
         rep.gbytes = per_site * ctx->g.Vh * 1e-9;
         rep.seconds = 0.0;

@@ -35,6 +35,37 @@ struct CgDevState {
   // whose |r|^2 is within this factor of its own (non-final) trigger pauses
   // with it, so that their updates coincide (1: off)
   double align;
+  // the reliable update's stopping rule (rel_stop) and its inputs
+  const double* bnorm;  // |b|
+  const int* upd;       // RHS in the current reliable update
+  int* cont;            // out: RHS of the update that go on
+  double tol;
+  int maxiter;
+};
+
+// Why a reliable update ends a RHS's solve, from its true residual |A r|^2
+// (|r|^2 without clover): REL_GO, it goes on. The residual |A r| / |b| is
+// left in *res.
+enum { REL_GO = 0, REL_CONV, REL_BREAK, REL_CAP };
+QCU_D int rel_stop(double ar2, double bn, int brk, int iters, double tol, int maxiter, double* res) {
+  *res = bn > 0 ? sqrt(fmax(ar2, 0.0)) / bn : 0.0;
+  if (bn == 0.0 || *res < tol) return REL_CONV;
+  if (!isfinite(*res) || brk) return REL_BREAK;
+  if (iters >= maxiter) return REL_CAP;
+  return REL_GO;
+}
+
+// Finishing functor of the true-residual reduction of a reliable update:
+// marks the RHS that go on, so that only they get r_ne.
+struct FinRelCont {
+  static QCU_D void apply(const double* res, int nrhs, int NR, void* st, int t, int nt) {
+    CgDevState* s = static_cast<CgDevState*>(st);
+    for (int r = t; r < nrhs; r += nt) {
+      double q;
+      s->cont[r] = s->upd[r] && rel_stop(res[r * NR], s->bnorm[r], s->breakdown[r], s->iters[r], s->tol,
+                                         s->maxiter, &q) == REL_GO;
+    }
+  }
 };
 
 // Every thread of the block calls apply (t = its index, nt = the block's

@@ -269,10 +269,12 @@ cudaError_t launch_accumulate_res(int pl, int nsites, int nrhs, SpinorView xhi, 
                                   SpinorView d, const int* active, LaunchShape sh, cudaStream_t st);
 // |A r|^2 per RHS (into red) and u = A^-1 r in one pass from the FP64 r, FP64
 // clover fields; u in precision pu, and for pu other than FP64 also r rounded
-// to pu into rs
+// to pu into rs. fin: FIN_NONE, or FIN_REL_CONT (red.state the CG state) to
+// mark the RHS that go on after the reliable update.
 cudaError_t launch_clover_res(int pu, const Geom& g, int parity, int nrhs, CSpinorView r, SpinorView u, SpinorView rs,
                               const void* A, const void* Ainv, size_t clov_stride, const int* clov_idx,
-                              const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t stream);
+                              const int* active, const ReduceArgs& red, LaunchShape sh, cudaStream_t stream,
+                              int fin = 0);
 cudaError_t launch_residual(int nsites, int nrhs, SpinorView r, CSpinorView b, CSpinorView z, const int* active,
                             const ReduceArgs& red, LaunchShape sh, cudaStream_t st);
 cudaError_t launch_cdot(int prec, int nsites, int nrhs, CSpinorView x, CSpinorView y, const int* active,

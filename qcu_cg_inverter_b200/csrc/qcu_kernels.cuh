@@ -62,7 +62,9 @@ struct DslashArgs {
 };
 
 // Finishing functors available to fused reductions (see solver kernels).
-enum FinId : int { FIN_NONE = 0, FIN_CG_ALPHA = 1, FIN_CG_BETA = 2 };
+// FIN_REL_CONT: marks the RHS that go on after a reliable update (the
+// residual reduction of clover_res, or a one-block launch; never a stencil's)
+enum FinId : int { FIN_NONE = 0, FIN_CG_ALPHA = 1, FIN_CG_BETA = 2, FIN_REL_CONT = 3 };
 
 // shared-memory bytes of NT staged neighbours (16-bit words and norms of both
 // lanes of every thread) of a block of RB/2 x SB threads (the RHS-paired

@@ -19,8 +19,10 @@ enum { D_RR = 0, D_RROLD, D_PAP, D_ALPHA, D_BETA, D_TRIG, D_KAPPA, D_MK2, D_K2, 
        D_BNORM, D_TRUE, D_RRPRE, D_NUM };  // D_MK2 = -kappa^2, D_K2 = +kappa^2
 // I_ADM: RHS being admitted (source staged, bhat and x = 0 to be set up);
 // I_RET: RHS being retired (solution reconstructed and copied out).
+// I_CONT: RHS of the current reliable update that go on iterating (the others
+// stop at it and need no r_ne).
 enum { I_ACTIVE = 0, I_EVENT, I_ITERS, I_BREAK, I_CIDX, I_UPD, I_RST, I_DONE, I_CONV, I_STATUS, I_NUPD, I_ADM, I_RET, I_FINAL,
-       I_NUM };
+       I_CONT, I_NUM };
 
 
 struct RelParams {
@@ -71,6 +73,7 @@ struct SolverWorkspace {
 // admission plus retirement of a column.
 double iteration_bytes(int op, bool clover, int share);
 double reliable_update_bytes(int op, bool clover, int share);
+double reliable_update_ne_bytes(int op, bool clover, int share);  // its r_ne part (not in a stopping update)
 double admit_retire_bytes(bool clover, int share);
 
 struct OpCtx {
@@ -82,6 +85,9 @@ struct OpCtx {
 
 
 int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clover, double align = 1.0);
+// The stopping rule of the reliable updates (tolerance, iteration cap) in the
+// device copy of the CG state.
+int ws_set_stop(qcu_context ctx, SolverWorkspace& w, double tol, int maxiter);
 DslashArgs op_args(const OpCtx& o, int prec, int parity, const Field& in, const Field& out, const int* mask);
 int dsl(const OpCtx& o, int prec, bool dag, int epi, int fin, const DslashArgs& a);
 ReduceArgs red_into(const OpCtx& o, double* result, bool with_state);

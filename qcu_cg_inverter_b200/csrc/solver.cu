@@ -56,22 +56,15 @@ __global__ void rel_decide_kernel(int nrhs, double* dmem, int* imem, RelParams P
   if (!IV(I_UPD)) return;
   IV(I_NUPD) += 1;
   double ar2 = P.clover ? DV(D_RES_AR2) : DV(D_RES_R2);
-  double ne2 = DV(D_RES_NE);
+  double ne2 = DV(D_RES_NE);  // computed only for the RHS that go on (I_CONT)
   double bn = DV(D_BNORM);
-  double res = bn > 0 ? sqrt(fmax(ar2, 0.0)) / bn : 0.0;
+  double res = 0.0;
+  const int why = rel_stop(ar2, bn, IV(I_BREAK), IV(I_ITERS), P.tol, P.maxiter, &res);
   DV(D_TRUE) = res;
-  int stop = 0;
-  if (bn == 0.0 || res < P.tol) {
-    IV(I_CONV) = 1;
-    stop = 1;
-  } else if (!isfinite(res) || IV(I_BREAK)) {
-    IV(I_STATUS) = QCU_ERR_BREAKDOWN;
-    stop = 1;
-  } else if (IV(I_ITERS) >= P.maxiter) {
-    IV(I_STATUS) = QCU_ERR_NOT_CONVERGED;
-    stop = 1;
-  }
-  if (stop) {
+  if (why == REL_CONV) IV(I_CONV) = 1;
+  else if (why == REL_BREAK) IV(I_STATUS) = QCU_ERR_BREAKDOWN;
+  else if (why == REL_CAP) IV(I_STATUS) = QCU_ERR_NOT_CONVERGED;
+  if (why != REL_GO) {
     IV(I_DONE) = 1;
     IV(I_ACTIVE) = 0;
     IV(I_EVENT) = 0;
@@ -109,13 +102,17 @@ double iteration_bytes(int op, bool clover, int share) {
   return k1 + k2 + k3 + k4 + k5;
 }
 
+double reliable_update_ne_bytes(int op, bool clover, int share) {
+  return iteration_bytes(op, clover, share) * 0.5;  // r_ne = Mhat^dag r, sloppy
+}
+
 double reliable_update_bytes(int op, bool clover, int share) {
   const double s64 = 192.0, l64 = 96.0, c64 = clover ? 576.0 : 0.0;
   const double hop64 = 8.0 * s64 + 8.0 * l64 / share;
   const double acc = sb_of(acc_prec(op_spinor_prec(op))) + 4.0 * s64;  // x_hi += x_lo, y = bhat - x_hi
   const double res = 2.0 * hop64 + 2.0 * c64 / share + 3.0 * s64;      // r = bhat - Mhat x_hi
   const double cres = s64 + 2.0 * c64 / share + 2.0 * sb_of(op_spinor_prec(op));
-  const double ne = iteration_bytes(op, clover, share) * 0.5;           // r_ne = Mhat^dag r, sloppy
+  const double ne = reliable_update_ne_bytes(op, clover, share);
   return acc + res + cres + ne;
 }
 
@@ -164,8 +161,18 @@ int ws_prepare(qcu_context ctx, SolverWorkspace& w, int nrhs, int ps, bool clove
   w.st.breakdown = w.di(I_BREAK);
   w.st.final_trig = w.di(I_FINAL);
   w.st.align = align;
+  w.st.bnorm = w.dd(D_BNORM);
+  w.st.upd = w.di(I_UPD);
+  w.st.cont = w.di(I_CONT);
   QCU_CHECK_CUDA(cudaMemcpyAsync(w.dstate.p, &w.st, sizeof(CgDevState), cudaMemcpyHostToDevice, st));
   QCU_CHECK(ctx->red.ensure(ctx->g, nrhs, st, w.shape.Sb));
+  return QCU_SUCCESS;
+}
+
+int ws_set_stop(qcu_context ctx, SolverWorkspace& w, double tol, int maxiter) {
+  w.st.tol = tol;
+  w.st.maxiter = maxiter;
+  QCU_CHECK_CUDA(cudaMemcpyAsync(w.dstate.p, &w.st, sizeof(CgDevState), cudaMemcpyHostToDevice, ctx->stream));
   return QCU_SUCCESS;
 }
 
@@ -223,6 +230,7 @@ __global__ void fin_kernel(const ReduceArgs red, int nrhs) {
 cudaError_t launch_fin(int fin, const ReduceArgs& red, int nrhs, cudaStream_t st) {
   if (fin == FIN_CG_ALPHA) fin_kernel<FinCgAlpha><<<1, 64, 0, st>>>(red, nrhs);
   else if (fin == FIN_CG_BETA) fin_kernel<FinCgBeta><<<1, 64, 0, st>>>(red, nrhs);
+  else if (fin == FIN_REL_CONT) fin_kernel<FinRelCont><<<1, 64, 0, st>>>(red, nrhs);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -321,24 +329,35 @@ int reliable_update(const OpCtx& o, bool fresh) {
   // (the restart then copies nothing; columns that stop are not read again)
   const bool ne_in_place = (sloppy_ne ? w.ps : PREC_DOUBLE) == w.pa;
   const Field& zn = ne_in_place ? w.rlo : (sloppy_ne ? w.z : w.z64);
+  // the RHS that go on after this update (I_CONT, by the decide kernel's
+  // stopping rule): only they need r_ne. On one slab with clover the residual
+  // reduction's finishing functor marks them; otherwise a one-block launch
+  // after the (rank-summed) residual.
+  const int* cont = w.di(I_CONT);
+  const bool cont_in_res = w.clover && !o.ctx->g.tdd;
   if (w.clover) {  // |A_ee r|^2 and u = A_ee^-1 r in one pass (and r, u rounded to the sloppy storage)
     QCU_CHECK_CUDA(launch_clover_res(sloppy_ne ? w.ps : PREC_DOUBLE, o.ctx->g, 0, w.nrhs,
                                      from_b ? w.bh.cview(0) : w.y64.cview(0),
                                      uin.view(0), w.y.view(0), ctx_clover_ptr(o.ctx, PREC_DOUBLE, false),
                                      ctx_clover_ptr(o.ctx, PREC_DOUBLE, true), ctx_clover_stride(o.ctx, PREC_DOUBLE),
-                                     w.di(I_CIDX), upd, red_into(o, w.dd(D_RES_AR2), false), w.shape, o.st));
+                                     w.di(I_CIDX), upd, red_into(o, w.dd(D_RES_AR2), cont_in_res), w.shape, o.st,
+                                     cont_in_res ? FIN_REL_CONT : FIN_NONE));
     o.ctx->launches++;
     QCU_CHECK(dd_sum(o.ctx, w.dd(D_RES_AR2), w.nrhs, o.st));
   } else if (sloppy_ne) {
     QCU_CHECK_CUDA(launch_convert(w.ps, PREC_DOUBLE, Vh, w.nrhs, w.y.view(0), w.y64.cview(0), upd, nullptr, w.shape, o.st));
     o.ctx->launches++;
   }
+  if (!cont_in_res) {
+    QCU_CHECK_CUDA(launch_fin(FIN_REL_CONT, red_into(o, w.dd(w.clover ? D_RES_AR2 : D_RES_R2), true), w.nrhs, o.st));
+    o.ctx->launches++;
+  }
   {
-    DslashArgs a = op_args(o, pn, 1, w.clover ? uin : rin, tn, upd);
+    DslashArgs a = op_args(o, pn, 1, w.clover ? uin : rin, tn, cont);
     QCU_CHECK(dsl(o, pn, true, w.clover ? EPI_CPRE : 0, FIN_NONE, a));
   }
   {
-    DslashArgs a = op_args(o, pn, 0, tn, zn, upd);
+    DslashArgs a = op_args(o, pn, 0, tn, zn, cont);
     a.x = rin.cview(0);
     a.coef = w.dd(D_MK2);
     a.red = red_into(o, w.dd(D_RES_NE), false);
